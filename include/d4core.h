@@ -1,0 +1,178 @@
+/*
+ * d4core.h: C ABI of the B200 engine for the 2D4_sim implicit-step hot path.
+ *
+ * Library: 2d4_b200/lib/libd4core.so (CUDA, sm_100a).  Plain C types only; every
+ * function returns an int status: D4_OK (0), D4_WARN_SINGULAR (1, mirrors
+ * UMFPACK_WARNING_singular_matrix) or a negative error.  Nothing crosses this
+ * boundary as an exception or an exit().  d4_last_error() gives the message of
+ * the last failure on a context.
+ *
+ * Positions are passed in the reference's internal order (sorted by y+b
+ * descending, src/simulation_data.cpp:116), so the Burgers vector of
+ * dislocation i is +1 for i < n/2 and -1 otherwise
+ * (src/simulation_data.cpp:265-270).  Host pointers are copied in and out;
+ * results are complete when a call returns.  A context is not thread-safe;
+ * separate contexts may be used from separate threads.
+ *
+ * What each entry point replaces in the reference (danieltuzes/2D4):
+ *   d4_speeds            Simulation::calculateSpeedsAtTime   src/simulation.cpp:287-333
+ *   d4_jacobian          Simulation::calcJacobianAndSpeedsAtTimes src/simulation.cpp:345-527
+ *   d4_jacobian_from_prev Simulation::calcJacobianAndSpeedsFromPrev src/simulation.cpp:546-608
+ *   d4_factor            calculateSparseFormForJacobian ->
+ *                        umfpack_di_symbolic/numeric     src/simulation.cpp:635-640
+ *   d4_solve             Simulation::solveEQSys -> umfpack_di_solve src/simulation.cpp:643-659
+ *   d4_attempt           stages I-III + calculateXError   src/simulation.cpp:90-161,692-700
+ *   d4_run               Simulation::run                  src/simulation.cpp:30-281
+ *   d4_field_xy / d4_field_xy_diff_x  Field::xy / Field::xy_diff_x src/Fields/Field.cpp:295-346
+ */
+#ifndef D4CORE_H
+#define D4CORE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    D4_OK = 0,
+    D4_WARN_SINGULAR = 1,
+    D4_ERR_ARG = -1,
+    D4_ERR_CUDA = -2,
+    D4_ERR_NOMEM = -3,
+    D4_ERR_STATE = -4,
+    D4_ERR_IO = -5
+};
+
+/* Arithmetic of the hot path. */
+enum {
+    D4_PREC_FP64 = 0,  /* plain form: FP64 throughout, reference operation order */
+    D4_PREC_MIXED = 1  /* FP32 pair sums + TF32 tensor-core LU + FP64 refinement */
+};
+
+/* External stress protocol (src/stress_protocol.cpp:13-73). */
+enum {
+    D4_STRESS_NONE = 0,        /* StressProtocol: always 0 (even with tau0, as -s alone) */
+    D4_STRESS_FIXED_RATE = 1,  /* FixedRateProtocol: tau0 + rate*t */
+    D4_STRESS_CYCLIC = 2,      /* CyclicLoadProtocol */
+    D4_STRESS_INC_CYCLIC = 3   /* IncreasingCyclicLoadProtocol */
+};
+
+typedef struct d4_protocol {
+    int kind;
+    double tau0;           /* initExtStress (-s) */
+    double rate;           /* m_rate (-r) */
+    double period;         /* m_timePeriod (-i) */
+    double amplitude_rate; /* m_amplitudeRate (-A) */
+} d4_protocol;
+
+/* The flags of src/project_parser.cpp:28-68 that the stepping loop reads. */
+typedef struct d4_params {
+    double position_precision;    /* -P, default 1e-5 */
+    double dipole_precision;      /* -p, default 0.05; 0 disables */
+    double cutoff_multiplier;     /* -u, default 1e20 (no cutoff) */
+    int heaviside_cutoff;         /* -h */
+    double initial_stepsize;      /* --initial-stepsize, default 1e-6 */
+    double max_stepsize;          /* -M; <= 0: none */
+    char weight_function;         /* -w: 'c' (default), 'p' or 'm' */
+    double time_limit;            /* -t; < 0: none */
+    long long step_count_limit;   /* -C; < 0: none (n stops after n+1 accepted steps) */
+    double strain_increase_limit; /* < 0: none */
+    int calculate_strain;         /* -S */
+    int calculate_order_parameter;/* -l */
+    long long avalanche_limit;    /* --avalanche-detection-limit; < 0: none */
+    double avalanche_speed_threshold; /* default 1e-3 */
+    int save_sub_configs;         /* -o given */
+    unsigned sub_config_delay;    /* -N, default 5 */
+    unsigned sub_config_delay_during_avalanche; /* -n, default 1 */
+    double sub_config_times;      /* -T; 0: none */
+    char sub_config_times_type;   /* -b: 'a' (default) or 'b' */
+    d4_protocol protocol;
+    int precision;                /* D4_PREC_FP64 or D4_PREC_MIXED */
+    int device;                   /* CUDA device ordinal */
+} d4_params;
+
+/* Result of one attempted step (stages I-IV before acceptance). */
+typedef struct d4_attempt_result {
+    double ratio;       /* PrecisionHandler::getMaxErrorRatioSqr() */
+    int max_id;         /* PrecisionHandler::maxErrorRatioID() */
+    int accepted;       /* ratio < 1 */
+    int singular;       /* a factorisation met an exact zero pivot */
+    int pivoted;        /* number of factorisations that needed row swaps */
+} d4_attempt_result;
+
+typedef struct d4_run_result {
+    double sim_time;
+    double step_size;
+    double strain;
+    double energy;
+    long long successful_steps;
+    long long failed_steps;
+    long long attempts;
+    long long pivoted_factorizations;
+    long long singular_factorizations;
+    double device_seconds; /* CUDA-event time of the stepping loop */
+} d4_run_result;
+
+/* Optional outputs of d4_run (all may be null). */
+typedef struct d4_run_io {
+    const char *log_path;          /* 15-column log, src/simulation.cpp:52-83,184-209 */
+    const char *sub_config_prefix; /* sub-configuration files prefix (-o) */
+    const char *end_config_path;   /* final configuration (-O) */
+    const unsigned *order;         /* original index -> internal index, for output */
+    long long max_attempts;        /* > 0: stop after this many attempts */
+} d4_run_io;
+
+void d4_default_params(d4_params *p);
+
+int d4_create(void **ctx, int n, const d4_params *p);
+int d4_destroy(void *ctx);
+const char *d4_last_error(void *ctx);
+
+int d4_set_positions(void *ctx, const double *x, const double *y);
+int d4_get_positions(void *ctx, double *x, double *y);
+int d4_set_time(void *ctx, double sim_time, double step_size);
+
+/* Stress sweep on positions x, y (host, length n) at sim_time.  v receives the
+ * speeds; tol (may be null) receives the per-dislocation tolerance after the
+ * sweep, starting from the context's current tolerances. */
+int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, double *v,
+              double *tol);
+
+/* Fused sweep: speeds at t_a and t_b, the scaled Jacobian A = I + D J kept on
+ * the device (and copied to a_colmajor when non-null), and dvec. */
+int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, double t_a,
+                double t_b, double *v_a, double *v_b, double *a_colmajor, double *dvec,
+                double *tol);
+
+/* Half-step rescale of the device Jacobian and dvec with
+ * factor = (t_new - t_base) / (t_old - t_base); a_colmajor/dvec may be null. */
+int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *dvec);
+
+/* Factorise the device Jacobian.  Returns D4_WARN_SINGULAR on an exact zero
+ * pivot, like umfpack_di_numeric. */
+int d4_factor(void *ctx);
+
+/* Solve A dx = g with the last factorisation (UMFPACK_A).  Returns
+ * D4_WARN_SINGULAR like umfpack_di_solve; the caller zeroes entries outside
+ * (-1, 1) as src/simulation.cpp:646-658 does (d4_attempt/d4_run do this). */
+int d4_solve(void *ctx, const double *g, double *dx);
+
+/* Reset the per-dislocation tolerances (PrecisionHandler::reset). */
+int d4_reset_tolerance(void *ctx);
+
+/* One attempted step from the context's positions at t0 with step h. The
+ * big-step and two half-step positions stay on the device (d4_get_attempt). */
+int d4_attempt(void *ctx, double t0, double h, d4_attempt_result *res);
+int d4_get_attempt(void *ctx, double *x_big, double *x_half, double *x_two);
+
+/* Simulation::run on the context's positions; positions are updated. */
+int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res);
+
+/* Single field evaluations on the device (FP64 path), for checks. */
+int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
+                  double *xy_diff_x);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
