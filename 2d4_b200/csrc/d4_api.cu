@@ -1,0 +1,603 @@
+// d4_api.cu: C ABI of libd4core.so and the host side of the stepping loop.
+//
+// The loop mirrors Simulation::run (src/simulation.cpp:30-281): the hot path
+// (pair sweeps, Jacobian, factorisations, solves, error reduction) runs on the
+// device; the scalar control (accept/reject, PrecisionHandler::getNewStepSize,
+// write-out clipping, stop conditions, log lines) runs here on the host in the
+// reference's own double arithmetic, with one 16-byte read-back per attempt.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "d4_internal.h"
+
+using d4::Ctx;
+using d4::CudaError;
+
+namespace {
+
+// StressProtocol family, src/stress_protocol.cpp:13-73.
+double ext_stress(const d4_protocol &p, double t) {
+    switch (p.kind) {
+    case D4_STRESS_FIXED_RATE:
+        return t * p.rate + p.tau0;
+    case D4_STRESS_CYCLIC:
+    case D4_STRESS_INC_CYCLIC: {
+        double periodic = t - std::floor((t / p.period + 1. / 4)) * p.period;
+        double stress = p.rate * periodic + p.tau0;
+        if (periodic > p.period / 4) stress = p.rate * p.period / 2 - stress + p.tau0;
+        if (p.kind == D4_STRESS_INC_CYCLIC) return stress * p.amplitude_rate * t;
+        return stress;
+    }
+    default:
+        return 0;
+    }
+}
+
+// SimulationData::getNextWriteOutTime, src/simulation_data.cpp:231-246.
+double next_write_out(const d4_params &p, double sim_time) {
+    if (p.sub_config_times == 0) return INFINITY;
+    if (p.sub_config_times_type == 'a')
+        return (double)((size_t)(sim_time / p.sub_config_times) + 1) * p.sub_config_times;
+    if (p.sub_config_times_type == 'b') {
+        double exponent =
+            std::nextafter(std::log(sim_time / p.initial_stepsize) / std::log(p.sub_config_times),
+                           INFINITY);
+        int next_exp = std::max((int)exponent + 1, 1);
+        return p.initial_stepsize * std::pow(p.sub_config_times, next_exp);
+    }
+    return INFINITY;
+}
+
+template <typename T>
+void dalloc(T **p, size_t count) {
+    D4_CUDA_OK(cudaMalloc((void **)p, sizeof(T) * (count > 0 ? count : 1)));
+}
+
+void free_all(Ctx *c) {
+    void *bufs[] = {c->x0, c->y, c->xb, c->xh, c->x2, c->xs_tmp, c->ys_tmp, c->v_init,
+                    c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
+                    c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (c->h_red) cudaFreeHost(c->h_red);
+    if (c->h_flags) cudaFreeHost(c->h_flags);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+int fail(Ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define D4_GUARD_BEGIN try {
+#define D4_GUARD_END(c)                                         \
+    }                                                           \
+    catch (const CudaError &e) {                                \
+        return fail((c), D4_ERR_CUDA, e.what);                  \
+    }                                                           \
+    catch (const std::bad_alloc &) {                            \
+        return fail((c), D4_ERR_NOMEM, "host allocation failed"); \
+    }
+
+void upload(Ctx &c, double *dst, const double *src) {
+    D4_CUDA_OK(cudaMemcpyAsync(dst, src, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream));
+}
+
+void download(Ctx &c, double *dst, const double *src) {
+    D4_CUDA_OK(cudaMemcpyAsync(dst, src, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));
+}
+
+void sync(Ctx &c) { D4_CUDA_OK(cudaStreamSynchronize(c.stream)); }
+
+// Stages I-IV of src/simulation.cpp:90-161 on the device.
+int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
+    const d4_protocol &pr = c.p.protocol;
+    const double t_1__ = t0 + h;
+    const double t_1p2 = t0 + h / 2;
+    int singular = 0, pivoted = 0, st;
+    // stage I: one large step
+    d4::jacobian64(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t_1__), c.v_init, c.speed);
+    st = d4::factor64(c);
+    singular |= st == D4_WARN_SINGULAR;
+    pivoted += c.factor_pivoted;
+    d4::solve_update64(c, d4::kGBig, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xb);
+    d4::speeds64(c, c.xb, c.y, ext_stress(pr, t_1__), c.speed2);
+    d4::solve_update64(c, d4::kGNewton, h, c.speed2, c.v_init, c.xb, c.x0, c.xb, c.xb);
+    // stage II: first small step, Jacobian from the previous one
+    {
+        const double factor = (t_1p2 - t0) / (t_1__ - t0);
+        d4::jacobian_from_prev64(c, factor);
+        st = d4::factor64(c);
+        singular |= st == D4_WARN_SINGULAR;
+        pivoted += c.factor_pivoted;
+        const double dif = ext_stress(pr, t_1p2) - ext_stress(pr, t_1__);
+        d4::shift_speed64(c, c.speed, dif);
+    }
+    d4::solve_update64(c, d4::kGHalf, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xh);
+    d4::speeds64(c, c.xh, c.y, ext_stress(pr, t_1p2), c.speed2);
+    d4::solve_update64(c, d4::kGNewton, h / 2, c.speed2, c.v_init, c.xh, c.x0, c.xh, c.xh);
+    // stage III: second small step
+    d4::jacobian64(c, c.xh, c.y, h / 2, ext_stress(pr, t_1p2), ext_stress(pr, t_1__), c.v_init2,
+                   c.speed2);
+    st = d4::factor64(c);
+    singular |= st == D4_WARN_SINGULAR;
+    pivoted += c.factor_pivoted;
+    d4::solve_update64(c, d4::kGHalf, h, c.speed2, c.v_init2, nullptr, nullptr, c.xh, c.x2);
+    d4::speeds64(c, c.x2, c.y, ext_stress(pr, t_1__), c.speed2);
+    d4::solve_update64(c, d4::kGNewton, h / 2, c.speed2, c.v_init2, c.x2, c.xh, c.x2, c.x2);
+    // stage IV: error ratio
+    d4::error_ratio64(c, c.xb, c.x2);
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost,
+                               c.stream));
+    sync(c);
+    const int idx = (int)c.h_red[1];
+    if (idx >= 0) c.selected_id = idx;
+    res->ratio = c.h_red[0] / c.dipole_prec_sq;
+    res->max_id = c.selected_id;
+    res->accepted = res->ratio < 1;
+    res->singular = singular;
+    res->pivoted = pivoted;
+    return D4_OK;
+}
+
+double host_abs_sum(const std::vector<double> &v) {
+    double s = 0;
+    for (double x : v) s = s + std::fabs(x);
+    return s;
+}
+
+double host_sq_sum(const std::vector<double> &v) {
+    double s = 0;
+    for (double x : v) s = s + x * x;
+    return s;
+}
+
+void write_config(Ctx &c, const std::string &path, const unsigned *order) {
+    std::vector<double> x(c.n), y(c.n);
+    download(c, x.data(), c.x0);
+    download(c, y.data(), c.y);
+    sync(c);
+    std::ofstream of(path);
+    if (!of) return;
+    // src/simulation_data.cpp:177-191: original order, 14 significant digits
+    of << std::setprecision(14);
+    for (int k = 0; k < c.n; ++k) {
+        const unsigned id = order ? order[k] : (unsigned)k;
+        of << x[id] << "\t" << y[id] << "\t" << (id < (unsigned)c.n / 2 ? 1 : -1) << "\n";
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void d4_default_params(d4_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->position_precision = 1e-5;
+    p->dipole_precision = 0.05;
+    p->cutoff_multiplier = 1e20;
+    p->initial_stepsize = 1e-6;
+    p->max_stepsize = -1;
+    p->weight_function = 'c';
+    p->time_limit = -1;
+    p->step_count_limit = -1;
+    p->strain_increase_limit = -1;
+    p->avalanche_limit = -1;
+    p->avalanche_speed_threshold = 1e-3;
+    p->sub_config_delay = 5;
+    p->sub_config_delay_during_avalanche = 1;
+    p->sub_config_times_type = 'a';
+    p->precision = D4_PREC_FP64;
+    p->device = 0;
+}
+
+int d4_create(void **out, int n, const d4_params *p) {
+    if (!out || !p) return D4_ERR_ARG;
+    *out = nullptr;
+    if (n < 2 || n % 2 != 0 || n > d4::kMaxSolveN) return D4_ERR_ARG;
+    if (p->weight_function != 'c' && p->weight_function != 'p' && p->weight_function != 'm')
+        return D4_ERR_ARG;
+    if (p->precision != D4_PREC_FP64) return D4_ERR_ARG;
+    Ctx *c = new (std::nothrow) Ctx();
+    if (!c) return D4_ERR_NOMEM;
+    try {
+        c->n = n;
+        c->p = *p;
+        D4_CUDA_OK(cudaSetDevice(p->device));
+        D4_CUDA_OK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        D4_CUDA_OK(cudaEventCreate(&c->ev0));
+        D4_CUDA_OK(cudaEventCreate(&c->ev1));
+        // PrecisionHandler::setMinPrecisity + setDipolePrecisity
+        // (src/precision_handler.cpp:65-89, src/simulation.cpp:24-26)
+        c->min_prec_sq = p->position_precision * p->position_precision;
+        if (p->dipole_precision == 0) {
+            c->use_dipole = 0;
+            c->dipole_prec_sq = 1;
+        } else {
+            c->use_dipole = 1;
+            c->dipole_prec_sq = p->dipole_precision * p->dipole_precision;
+            c->min_prec_sq /= p->dipole_precision * p->dipole_precision;
+        }
+        // SimulationData::updateCutOff, src/simulation_data.cpp:253-262
+        double mult = p->cutoff_multiplier;
+        if (!p->heaviside_cutoff && p->cutoff_multiplier >= std::sqrt(2 * (double)n) / 12)
+            mult = 1e20;
+        c->cutoff = mult / std::sqrt((double)n);
+        c->cutoff_sq = c->cutoff * c->cutoff;
+        c->range_sq = p->heaviside_cutoff ? 1 : 49;
+        c->step_size = p->initial_stepsize;
+        const size_t nn = (size_t)n * n;
+        double **vecs[] = {&c->x0, &c->y, &c->xb, &c->xh, &c->x2, &c->xs_tmp, &c->ys_tmp,
+                           &c->v_init, &c->v_init2, &c->speed, &c->speed2, &c->dvec,
+                           &c->dvec_new, &c->fac, &c->dx, &c->tol};
+        for (double **v : vecs) dalloc(v, (size_t)n);
+        dalloc(&c->A, nn);
+        dalloc(&c->LU, nn);
+        dalloc(&c->F, nn);
+        dalloc(&c->piv, (size_t)n);
+        dalloc(&c->perm, (size_t)n);
+        dalloc(&c->flags, (size_t)d4::kFlagCount);
+        dalloc(&c->red, 8);
+        D4_CUDA_OK(cudaMallocHost((void **)&c->h_red, sizeof(double) * 8));
+        D4_CUDA_OK(cudaMallocHost((void **)&c->h_flags, sizeof(int) * d4::kFlagCount));
+        D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
+        D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
+        D4_CUDA_OK(cudaMemset(c->dvec, 0, sizeof(double) * n));
+        D4_CUDA_OK(cudaMemset(c->flags, 0, sizeof(int) * d4::kFlagCount));
+        d4::init_lu64();
+        d4::reset_tol64(*c);
+        sync(*c);
+    } catch (const CudaError &e) {
+        free_all(c);
+        delete c;
+        return D4_ERR_CUDA;
+    }
+    *out = c;
+    return D4_OK;
+}
+
+int d4_destroy(void *ctx) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return D4_OK;
+}
+
+const char *d4_last_error(void *ctx) {
+    Ctx *c = (Ctx *)ctx;
+    return c ? c->err.c_str() : "null context";
+}
+
+int d4_set_positions(void *ctx, const double *x, const double *y) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !x || !y) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    upload(*c, c->x0, x);
+    upload(*c, c->y, y);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_get_positions(void *ctx, double *x, double *y) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !x) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    download(*c, x, c->x0);
+    if (y) download(*c, y, c->y);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_set_time(void *ctx, double sim_time, double step_size) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    c->sim_time = sim_time;
+    c->step_size = step_size;
+    return D4_OK;
+}
+
+int d4_reset_tolerance(void *ctx) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    d4::reset_tol64(*c);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, double *v,
+              double *tol) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !x || !y || !v) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    upload(*c, c->xs_tmp, x);
+    upload(*c, c->ys_tmp, y);
+    d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
+    download(*c, v, c->speed2);
+    if (tol) download(*c, tol, c->tol);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, double t_a,
+                double t_b, double *v_a, double *v_b, double *a_colmajor, double *dvec,
+                double *tol) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !x || !y || !v_a || !v_b) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    upload(*c, c->xs_tmp, x);
+    upload(*c, c->ys_tmp, y);
+    d4::jacobian64(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
+                   ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
+    download(*c, v_a, c->v_init);
+    download(*c, v_b, c->speed);
+    if (dvec) download(*c, dvec, c->dvec);
+    if (tol) download(*c, tol, c->tol);
+    if (a_colmajor)
+        D4_CUDA_OK(cudaMemcpyAsync(a_colmajor, c->A, sizeof(double) * (size_t)c->n * c->n,
+                                   cudaMemcpyDeviceToHost, c->stream));
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *dvec) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    d4::jacobian_from_prev64(*c, factor);
+    if (dvec) download(*c, dvec, c->dvec);
+    if (a_colmajor)
+        D4_CUDA_OK(cudaMemcpyAsync(a_colmajor, c->A, sizeof(double) * (size_t)c->n * c->n,
+                                   cudaMemcpyDeviceToHost, c->stream));
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_set_matrix(void *ctx, const double *a_colmajor) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !a_colmajor) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    D4_CUDA_OK(cudaMemcpyAsync(c->A, a_colmajor, sizeof(double) * (size_t)c->n * c->n,
+                               cudaMemcpyHostToDevice, c->stream));
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_factor(void *ctx) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    return d4::factor64(*c);
+    D4_GUARD_END(c)
+}
+
+int d4_solve(void *ctx, const double *g, double *dx) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !g || !dx) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    upload(*c, c->xs_tmp, g);
+    d4::solve_plain64(*c, c->xs_tmp);
+    download(*c, dx, c->dx);
+    sync(*c);
+    return c->factor_singular ? D4_WARN_SINGULAR : D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_attempt(void *ctx, double t0, double h, d4_attempt_result *res) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !res) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    return attempt(*c, t0, h, res);
+    D4_GUARD_END(c)
+}
+
+int d4_get_attempt(void *ctx, double *x_big, double *x_half, double *x_two) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    if (x_big) download(*c, x_big, c->xb);
+    if (x_half) download(*c, x_half, c->xh);
+    if (x_two) download(*c, x_two, c->x2);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
+                  double *xyd) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || count < 0 || !dx || !dy || !xy || !xyd) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    double *d = nullptr;
+    D4_CUDA_OK(cudaMalloc((void **)&d, sizeof(double) * 4 * (size_t)(count > 0 ? count : 1)));
+    const size_t b = sizeof(double) * (size_t)count;
+    cudaMemcpyAsync(d, dx, b, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d + count, dy, b, cudaMemcpyHostToDevice, c->stream);
+    d4::field_eval64(*c, count, d, d + count, d + 2 * count, d + 3 * count);
+    cudaMemcpyAsync(xy, d + 2 * count, b, cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(xyd, d + 3 * count, b, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    D4_CUDA_OK(e);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+// Simulation::run, src/simulation.cpp:30-281.
+int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    const d4_params &p = c->p;
+    const int n = c->n;
+    d4_run_io none{};
+    if (!io) io = &none;
+    std::ofstream log;
+    if (io->log_path && *io->log_path) {
+        log.open(io->log_path);
+        if (!log) return fail(c, D4_ERR_IO, std::string("cannot open log ") + io->log_path);
+        log << std::scientific << std::setprecision(16);
+    }
+    const bool want_log = log.is_open();
+    std::vector<double> hv(n), hv2(n), hv3(n);
+    double strain = 0, energy = 0, h_before_writeout = 0;
+    long long ok = 0, failed = 0, attempts = 0, n_piv = 0, n_sing = 0;
+    long long aval_count = 0;
+    bool in_aval = false;
+    unsigned sub_counter = 0;
+    double next_wo = p.save_sub_configs ? next_write_out(p, c->sim_time) : INFINITY;
+    double *d_strain = c->red + 4;
+
+    D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
+    // src/simulation.cpp:46: initial speeds (also seeds the tolerances)
+    d4::speeds64(*c, c->x0, c->y, ext_stress(p.protocol, c->sim_time), c->v_init);
+    if (want_log) {
+        download(*c, hv.data(), c->v_init);
+        sync(*c);
+        const double sum_avg = host_abs_sum(hv) / n;
+        log << "# simTime(1)\tsuccessfullSteps(2)\tfailedSteps(3)\tmaxErrorRatioSqr(4)\t"
+               "maxErrorRatioID(5)\tsumAvgSp(6)\tcutOff(7)\torderParameter(8)\t"
+               "externalStress(9)\ttimeStageI - III(10)\tstrain(11)\tvSquare(12)\t"
+               "energy(13)\twallTimeElapsed(14)\tstepSize(15)\t\n";
+        log << c->sim_time << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t" << sum_avg
+            << "\t" << c->cutoff << "\t-\t" << ext_stress(p.protocol, c->sim_time) << "\t-\t"
+            << strain << "\t" << host_sq_sum(hv) << "\t" << energy << "\t" << 0 << "\t"
+            << c->step_size << "\n";
+    }
+    for (;;) {
+        // interrupt(), src/simulation.cpp:722-750
+        if (p.time_limit >= 0 && c->sim_time > p.time_limit) break;
+        if (p.strain_increase_limit >= 0 && strain > p.strain_increase_limit) break;
+        if (p.step_count_limit >= 0 && ok > p.step_count_limit) break;
+        if (p.avalanche_limit >= 0 && aval_count > p.avalanche_limit) break;
+        if (io->max_attempts > 0 && attempts >= io->max_attempts) break;
+
+        const double h = c->step_size;
+        d4_attempt_result ar;
+        attempt(*c, c->sim_time, h, &ar);
+        ++attempts;
+        n_piv += ar.pivoted;
+        n_sing += ar.singular;
+        if (ar.ratio < 1) {
+            c->sim_time += h;
+            ++ok;
+            if (p.calculate_strain) {
+                d4::strain_increment64(*c, c->x0, c->xh, d_strain);
+                d4::strain_increment64(*c, c->xh, c->x2, d_strain + 1);
+                D4_CUDA_OK(cudaMemcpyAsync(c->h_red + 4, d_strain, sizeof(double) * 2,
+                                           cudaMemcpyDeviceToHost, c->stream));
+                sync(*c);
+                strain += c->h_red[4];
+                strain += c->h_red[5];
+            }
+            d4::normalize64(*c, c->x0, c->x2);
+            const bool need_speed = want_log || p.avalanche_limit >= 0;
+            double sum_avg = 0;
+            if (need_speed) {
+                download(*c, hv2.data(), c->v_init2);
+                sync(*c);
+                sum_avg = host_abs_sum(hv2) / n;
+            }
+            if (want_log) {
+                download(*c, hv.data(), c->v_init);
+                download(*c, hv3.data(), c->speed2);
+                sync(*c);
+                const double vsq_end = host_sq_sum(hv3);
+                energy += (host_sq_sum(hv) + 2 * host_sq_sum(hv2) + vsq_end) * h / 4;
+                log << c->sim_time << "\t" << ok << "\t" << failed << "\t" << ar.ratio << "\t"
+                    << ar.max_id << "\t" << sum_avg << "\t" << c->cutoff << "\t";
+                if (p.calculate_order_parameter) {
+                    download(*c, hv3.data(), c->speed);
+                    sync(*c);
+                    double op = 0;
+                    for (int i = 0; i < n; ++i) op += (i < n / 2 ? 1 : -1) * hv3[i];
+                    log << op << "\t";
+                } else
+                    log << "-\t";
+                log << ext_stress(p.protocol, c->sim_time) << "\t" << 0 << "\t";
+                if (p.calculate_strain)
+                    log << strain << "\t";
+                else
+                    log << "-\t";
+                log << vsq_end << "\t" << energy << "\t" << 0 << "\t" << h << "\n";
+            }
+            if (p.avalanche_limit >= 0) {
+                if (in_aval && sum_avg < p.avalanche_speed_threshold) {
+                    ++aval_count;
+                    in_aval = false;
+                } else if (sum_avg > p.avalanche_speed_threshold)
+                    in_aval = true;
+            }
+            if (p.save_sub_configs) {
+                if ((!in_aval && p.sub_config_delay <= sub_counter) ||
+                    (in_aval && p.sub_config_delay_during_avalanche <= sub_counter) ||
+                    next_wo <= c->sim_time) {
+                    sub_counter = 0;
+                    next_wo = next_write_out(p, c->sim_time);
+                    if (io->sub_config_prefix) {
+                        std::stringstream ss;
+                        ss << std::setprecision(9) << c->sim_time;
+                        write_config(*c, std::string(io->sub_config_prefix) + ss.str() + ".dconf",
+                                     io->order);
+                    }
+                } else
+                    ++sub_counter;
+            }
+        } else
+            ++failed;
+        // PrecisionHandler::getNewStepSize (src/precision_handler.cpp:57-62) and
+        // the write-out clipping of src/simulation.cpp:253-274
+        double hn = 0.9 * h * std::min(2., std::pow(ar.ratio, -1. / 6));
+        if (h_before_writeout != 0) {
+            if (ar.ratio < 1) hn = std::max(hn, h_before_writeout);
+            h_before_writeout = 0;
+        }
+        const double rem = std::nextafter(next_wo, INFINITY) - c->sim_time;
+        if (rem < hn) {
+            h_before_writeout = hn;
+            hn = rem;
+        }
+        if (c->use_dipole) d4::reset_tol64(*c);
+        if (p.max_stepsize > 0 && p.max_stepsize < hn) hn = p.max_stepsize;
+        c->step_size = hn;
+    }
+    D4_CUDA_OK(cudaEventRecord(c->ev1, c->stream));
+    sync(*c);
+    float ms = 0;
+    D4_CUDA_OK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (io->end_config_path) write_config(*c, io->end_config_path, io->order);
+    if (res) {
+        res->sim_time = c->sim_time;
+        res->step_size = c->step_size;
+        res->strain = strain;
+        res->energy = energy;
+        res->successful_steps = ok;
+        res->failed_steps = failed;
+        res->attempts = attempts;
+        res->pivoted_factorizations = n_piv;
+        res->singular_factorizations = n_sing;
+        res->device_seconds = ms / 1000.0;
+    }
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+}  // extern "C"

@@ -1,0 +1,361 @@
+// d4_fp64.cu: FP64 pair sweeps of the plain form (compiled with --fmad=false).
+//
+// Design.  The reference visits each unordered pair (i, j), i < j, once and
+// scatters its force antisymmetrically (src/simulation.cpp:292-311,444-483), so
+// speed i is the sum, in the order j = 0..n-1 (j != i), of -f(j,i) for j < i and
+// +f(i,j) for j > i, plus tau_ext*b_i.  Here a 2-D grid of 32x32 pair tiles
+// (upper triangle only, so each pair is evaluated once, like the reference)
+// evaluates the field and writes the signed pair force into an n x n matrix F
+// (column-major, transposed half via shared memory so both halves store
+// coalesced), and, in the fused sweep, the raw Jacobian entry into A.  A second
+// kernel with one thread per row then sums row i of F and of A in ascending j,
+// which reproduces the reference's summation order exactly, computes d_i and
+// applies the row scaling A = I + D J.  The per-dislocation nearest distance
+// (PrecisionHandler::updateTolerance) is a min, reduced with 64-bit atomicMin on
+// the bit pattern of the non-negative distance.
+#include <cstdint>
+
+#include "d4_field64.cuh"
+#include "d4_internal.h"
+
+namespace d4 {
+namespace {
+
+__device__ __forceinline__ double bsign(int i, int n) { return i < n / 2 ? 1.0 : -1.0; }
+
+__device__ __forceinline__ void tol_min(double *tol, int idx, double d) {
+    // d >= 0 here, so the IEEE bit patterns order like the values.
+    atomicMin(reinterpret_cast<unsigned long long *>(tol + idx),
+              static_cast<unsigned long long>(__double_as_longlong(d)));
+}
+
+// Enumerates upper-triangular tiles (ti <= tj) from a linear block index.
+__device__ __forceinline__ void tile_of(int t, int T, int &ti, int &tj) {
+    // row ti holds T - ti tiles; walk rows (T is small: <= 256 for n <= 8192)
+    int r = 0;
+    int rem = t;
+    while (rem >= T - r) {
+        rem -= T - r;
+        ++r;
+    }
+    ti = r;
+    tj = r + rem;
+}
+
+struct PairArgs {
+    int n;
+    const double *x, *y;
+    double *F;      // signed pair forces, column-major
+    double *A;      // raw Jacobian entries (fused sweep only)
+    double *tol;    // tolerance (may be null)
+    double min_prec_sq;
+    double h;       // step size of the Jacobian
+    double cut_sq, cutoff, range_sq, one_per_cut_sq;
+    int heaviside;
+};
+
+// One 32x32 tile of pairs per block; threadIdx.x = local i (coalesced column
+// stores), threadIdx.y steps local j.
+template <bool kJac>
+__global__ void __launch_bounds__(256) k_pairs64(PairArgs a) {
+    const int T = (a.n + kTile - 1) / kTile;
+    int ti, tj;
+    tile_of(blockIdx.x, T, ti, tj);
+    __shared__ double sxi[kTile], syi[kTile], sxj[kTile], syj[kTile];
+    __shared__ double sf[kTile][kTile + 1];
+    __shared__ double sv[kJac ? kTile : 1][kJac ? kTile + 1 : 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = ti * kTile, j0 = tj * kTile;
+    if (ty == 0) {
+        int i = i0 + tx, j = j0 + tx;
+        sxi[tx] = i < a.n ? a.x[i] : 0;
+        syi[tx] = i < a.n ? a.y[i] : 0;
+        sxj[tx] = j < a.n ? a.x[j] : 0;
+        syj[tx] = j < a.n ? a.y[j] : 0;
+    }
+    __syncthreads();
+    const int i = i0 + tx;
+    const double bi = bsign(i, a.n);
+    double row_min = 1e300;
+    for (int lj = ty; lj < kTile; lj += blockDim.y) {
+        const int j = j0 + lj;
+        double f = 0, v = 0;
+        if (i < a.n && j < a.n && i < j) {
+            double dx = f64::normalize(sxi[tx] - sxj[lj]);
+            double dy = f64::normalize(syi[tx] - syj[lj]);
+            double dist_sq = dx * dx + dy * dy;
+            if (a.tol && dist_sq < a.min_prec_sq) {
+                row_min = fmin(row_min, dist_sq);
+                tol_min(a.tol, j, dist_sq);
+            }
+            const double bj = bsign(j, a.n);
+            f64::Hyp hp(f64::exp2pix(dx));
+            double c = f64::cos2piy(dy);
+            f = f64::xy(dx, dy, hp, c) * bi * bj;
+            if (kJac) {
+                if (dist_sq < a.range_sq * a.cut_sq) {
+                    v = a.h * bj * bi * f64::xy_diff_x(dx, dy, hp, c);
+                    if (!a.heaviside && dist_sq > a.cut_sq) {
+                        double t = sqrt(dist_sq) - a.cutoff;
+                        v *= exp(-(t * t) * a.one_per_cut_sq);
+                    }
+                }
+            }
+            a.F[(size_t)i + (size_t)j * a.n] = f;
+            if (kJac) a.A[(size_t)i + (size_t)j * a.n] = v;
+        }
+        sf[tx][lj] = f;
+        if (kJac) sv[tx][lj] = v;
+    }
+    if (a.tol && i < a.n && row_min < a.min_prec_sq) tol_min(a.tol, i, row_min);
+    __syncthreads();
+    // transposed half: row j gets -f(i, j) at column i; lanes now walk j
+    const int j = j0 + tx;
+    for (int li = ty; li < kTile; li += blockDim.y) {
+        const int ii = i0 + li;
+        if (ii < a.n && j < a.n && ii < j) {
+            a.F[(size_t)j + (size_t)ii * a.n] = -sf[li][tx];
+            if (kJac) a.A[(size_t)j + (size_t)ii * a.n] = sv[li][tx];
+        }
+    }
+}
+
+// Ordered row sums of the stress sweep: v_i = sum_j F[i, j] + ext * b_i.
+__global__ void k_rows_speed64(int n, const double *__restrict__ F, double ext, double *v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0;
+    const double *col = F + i;
+    for (int j = 0; j < n; ++j)
+        if (j != i) s += col[(size_t)j * n];
+    v[i] = s + ext * bsign(i, n);
+}
+
+// Ordered row sums of the fused sweep and the row scaling
+// (src/simulation.cpp:503-522): A[i,i] = subSum, d_i = weight(subSum),
+// row i scaled by (1 + d_i)/2, +1 on the diagonal.
+__global__ void k_rows_jac64(int n, const double *__restrict__ F, double *A, double ext_a,
+                             double ext_b, double *v_a, double *v_b, double *dvec, char wfn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0, sub = 0;
+    for (int j = 0; j < n; ++j) {
+        if (j == i) continue;
+        s += F[(size_t)i + (size_t)j * n];
+        sub -= A[(size_t)i + (size_t)j * n];
+    }
+    const double b = bsign(i, n);
+    v_b[i] = s + ext_b * b;
+    v_a[i] = s + ext_a * b;
+    const double d = f64::weight(sub, wfn);
+    dvec[i] = d;
+    const double sc = (1 + d) / 2;
+    for (int j = 0; j < n; ++j) {
+        double *e = A + (size_t)i + (size_t)j * n;
+        if (j == i)
+            *e = sub * sc + 1;
+        else
+            *e = *e * sc;
+    }
+}
+
+// calcJacobianAndSpeedsFromPrev weights (src/simulation.cpp:552-582).
+__global__ void k_half_weights64(int n, const double *dvec, double factor, char wfn,
+                                 double *dnew, double *fac) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double old = dvec[i];
+    double w = 0.;
+    if (old != 0) w = f64::weight(f64::weight_inv(old, wfn) * factor, wfn);
+    dnew[i] = w;
+    fac[i] = (1 + w) / (1 + old);
+}
+
+// Elementwise rescale (src/simulation.cpp:584-594): factor of the row.
+__global__ void k_half_rescale64(int n, double *A, const double *fac) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)n * n;
+    if (idx >= total) return;
+    const int r = (int)(idx % n), c = (int)(idx / n);
+    const double f = fac[r];
+    double e = A[idx];
+    A[idx] = (r == c) ? 1 + (e - 1) / 2 * f : e / 2 * f;
+}
+
+__global__ void k_shift_speed64(int n, double *v, double dif) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] += dif * bsign(i, n);
+}
+
+__global__ void k_fill64(int n, double *v, double val) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = val;
+}
+
+// calculateXError + updateMaxErrorToleranceRatioSq (src/simulation.cpp:692-700,
+// src/precision_handler.cpp:41-54): max of err^2/tol with the first index
+// winning ties; out[0] = max, out[1] = index (or -1 when no value beats 0).
+__global__ void __launch_bounds__(1024) k_error_ratio64(int n, const double *xb, const double *x2,
+                                                        const double *tol, double min_prec_sq,
+                                                        int use_dipole, double *out) {
+    __shared__ double sv[32];
+    __shared__ int si[32];
+    double best = 0;
+    int bi = -1;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double e = fabs(xb[i] - x2[i]);
+        double t = use_dipole ? e * e / tol[i] : e * e / min_prec_sq;
+        if (t > best) {
+            best = t;
+            bi = i;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_down_sync(0xffffffffu, best, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (oi >= 0 && (ov > best || (ov == best && (bi < 0 || oi < bi)))) {
+            best = ov;
+            bi = oi;
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sv[w] = best;
+        si[w] = bi;
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        best = l < nw ? sv[l] : 0;
+        bi = l < nw ? si[l] : -1;
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, best, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (oi >= 0 && (ov > best || (ov == best && (bi < 0 || oi < bi)))) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (l == 0) {
+            out[0] = best;
+            out[1] = bi;
+        }
+    }
+}
+
+__global__ void k_normalize64(int n, double *dst, const double *src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = f64::normalize(src[i]);
+}
+
+// calculateStrainIncrement (src/simulation.cpp:713-720), sequential order.
+__global__ void k_strain64(int n, const double *old, const double *nw, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double r = 0;
+    for (int i = 0; i < n; ++i) r += bsign(i, n) * (nw[i] - old[i]);
+    *out = r;
+}
+
+// Field::xy (2-arg, exp2) and Field::xy_diff_x (2-arg, exp) at given points.
+__global__ void k_field64(int count, const double *dx, const double *dy, double *xy,
+                          double *xyd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const double x = dx[k], y = dy[k];
+    const double c = f64::cos2piy(y);
+    f64::Hyp h2(f64::exp2pix(x));
+    xy[k] = f64::xy(x, y, h2, c);
+    f64::Hyp he(exp(f64::kPi * 2 * x));
+    xyd[k] = f64::xy_diff_x(x, y, he, c);
+}
+
+inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+static PairArgs pair_args(Ctx &c, const double *x, const double *y) {
+    PairArgs a;
+    a.n = c.n;
+    a.x = x;
+    a.y = y;
+    a.F = c.F;
+    a.A = c.A;
+    a.tol = c.use_dipole ? c.tol : nullptr;
+    a.min_prec_sq = c.min_prec_sq;
+    a.h = 0;
+    a.cut_sq = c.cutoff_sq;
+    a.cutoff = c.cutoff;
+    a.range_sq = c.range_sq;
+    a.one_per_cut_sq = 1 / c.cutoff_sq;
+    a.heaviside = c.p.heaviside_cutoff;
+    return a;
+}
+
+static int pair_blocks(int n) {
+    const int T = (n + kTile - 1) / kTile;
+    return T * (T + 1) / 2;
+}
+
+void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v) {
+    PairArgs a = pair_args(c, x, y);
+    k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    check_launch("k_pairs64<speeds>");
+    k_rows_speed64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.F, ext, v);
+    check_launch("k_rows_speed64");
+}
+
+void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
+                double *v_a, double *v_b) {
+    PairArgs a = pair_args(c, x, y);
+    a.h = h;
+    k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    check_launch("k_pairs64<jacobian>");
+    k_rows_jac64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.F, c.A, ext_a, ext_b, v_a, v_b,
+                                                         c.dvec, c.p.weight_function);
+    check_launch("k_rows_jac64");
+}
+
+void jacobian_from_prev64(Ctx &c, double factor) {
+    k_half_weights64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.dvec, factor,
+                                                             c.p.weight_function, c.dvec_new,
+                                                             c.fac);
+    check_launch("k_half_weights64");
+    k_half_rescale64<<<blocks((long long)c.n * c.n, 256), 256, 0, c.stream>>>(c.n, c.A, c.fac);
+    check_launch("k_half_rescale64");
+    D4_CUDA_OK(cudaMemcpyAsync(c.dvec, c.dvec_new, sizeof(double) * c.n, cudaMemcpyDeviceToDevice,
+                               c.stream));
+}
+
+void shift_speed64(Ctx &c, double *v, double dif) {
+    k_shift_speed64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, v, dif);
+    check_launch("k_shift_speed64");
+}
+
+void reset_tol64(Ctx &c) {
+    k_fill64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.tol, c.min_prec_sq);
+    check_launch("k_fill64");
+}
+
+void error_ratio64(Ctx &c, const double *xb, const double *x2) {
+    k_error_ratio64<<<1, 1024, 0, c.stream>>>(c.n, xb, x2, c.tol, c.min_prec_sq, c.use_dipole,
+                                              c.red);
+    check_launch("k_error_ratio64");
+}
+
+void normalize64(Ctx &c, double *dst, const double *src) {
+    k_normalize64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, dst, src);
+    check_launch("k_normalize64");
+}
+
+void strain_increment64(Ctx &c, const double *x_old, const double *x_new, double *out) {
+    k_strain64<<<1, 32, 0, c.stream>>>(c.n, x_old, x_new, out);
+    check_launch("k_strain64");
+}
+
+void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double *xy,
+                  double *xyd) {
+    k_field64<<<blocks(count, 128), 128, 0, c.stream>>>(count, dx, dy, xy, xyd);
+    check_launch("k_field64");
+}
+
+}  // namespace d4

@@ -1,0 +1,108 @@
+// d4_internal.h: device state and kernel entry points shared by the
+// translation units of libd4core.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "d4core.h"
+
+namespace d4 {
+
+constexpr int kTile = 32;          // pair tile edge
+constexpr int kLuNb = 32;          // LU block width (FP64 path)
+constexpr int kSolveThreads = 1024;
+constexpr int kMaxSolveN = 8192;   // x and g of the one-CTA solve live in shared memory
+
+// Device flag words (ints in one small buffer).
+enum FlagSlot {
+    kFlagNeedPivot = 0,  // fast LU met |a_ik| > |a_kk| or a_kk == 0: partial pivoting would swap
+    kFlagSingular = 1,   // pivoted LU met an exact zero pivot
+    kFlagCount = 8
+};
+
+struct Ctx {
+    int n = 0;
+    d4_params p{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+
+    // derived scalars (host, reference rounding)
+    double min_prec_sq = 0, dipole_prec_sq = 1;
+    int use_dipole = 0;
+    double cutoff = 0, cutoff_sq = 0, range_sq = 49;
+
+    // host-side state of the stepping loop
+    double sim_time = 0, step_size = 0;
+    int selected_id = 0;
+    int factor_singular = 0;
+    int factor_pivoted = 0;
+    int lu_pivoted_path = 0;  // current factorisation came from the pivoted kernels
+
+    // device buffers (FP64)
+    double *x0 = nullptr, *y = nullptr, *xb = nullptr, *xh = nullptr, *x2 = nullptr;
+    double *xs_tmp = nullptr, *ys_tmp = nullptr;  // staging for d4_speeds / d4_jacobian
+    double *v_init = nullptr, *v_init2 = nullptr, *speed = nullptr, *speed2 = nullptr;
+    double *dvec = nullptr, *dvec_new = nullptr, *fac = nullptr, *dx = nullptr, *tol = nullptr;
+    double *A = nullptr;   // scaled Jacobian, column-major n x n
+    double *LU = nullptr;  // factorisation of A, column-major
+    double *F = nullptr;   // signed pair-force matrix (column-major) of one sweep
+    int *piv = nullptr, *perm = nullptr;
+    int *flags = nullptr;
+    double *red = nullptr;  // reduction results
+    // pinned host mirror of the small results
+    double *h_red = nullptr;
+    int *h_flags = nullptr;
+};
+
+// ---- FP64 pair sweeps (d4_fp64.cu) ----
+// Stress sweep: F (signed pair forces) and tolerance update, then ordered row sums.
+void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v);
+// Fused sweep: F and raw J, row sums, dvec, scaling to A = I + D J.
+void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
+                double *v_a, double *v_b);
+void jacobian_from_prev64(Ctx &c, double factor);
+void shift_speed64(Ctx &c, double *v, double dif);
+void reset_tol64(Ctx &c);
+void error_ratio64(Ctx &c, const double *xb, const double *x2);  // -> red[0], red[1]
+void normalize64(Ctx &c, double *x_dst, const double *x_src);
+void strain_increment64(Ctx &c, const double *x_old, const double *x_new, double *out);
+void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double *xy,
+                  double *xyd);
+
+// ---- FP64 factorisation and solves (d4_lu64.cu) ----
+// Factorises A into LU; returns via flags whether the pivoted path ran and
+// whether the matrix is singular.  Host-synchronising.
+int factor64(Ctx &c);
+void init_lu64();  // once per process and device, before the first solve
+enum GMode { kGBig = 0, kGHalf = 1, kGNewton = 2 };
+// g built from (gmode, hval, dvec, s_end, s_init, x_new, x_old); solve; out = base - dx.
+void solve_update64(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
+                    const double *x_new, const double *x_old, const double *base, double *out);
+// Plain solve of A dx = g (g on device, dx written to c.dx).
+void solve_plain64(Ctx &c, const double *g);
+
+}  // namespace d4
+
+#define D4_CUDA_OK(expr)                                                       \
+    do {                                                                       \
+        cudaError_t e_ = (expr);                                               \
+        if (e_ != cudaSuccess) throw d4::CudaError(e_, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+namespace d4 {
+struct CudaError {
+    cudaError_t code;
+    std::string what;
+    CudaError(cudaError_t c, const char *expr, const char *file, int line)
+        : code(c),
+          what(std::string(cudaGetErrorString(c)) + " at " + file + ":" + std::to_string(line) +
+               " (" + expr + ")") {}
+};
+inline void check_launch(const char *name) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError(e, name, __FILE__, __LINE__);
+}
+}  // namespace d4

@@ -18,12 +18,13 @@
  *   d4_speeds            Simulation::calculateSpeedsAtTime   src/simulation.cpp:287-333
  *   d4_jacobian          Simulation::calcJacobianAndSpeedsAtTimes src/simulation.cpp:345-527
  *   d4_jacobian_from_prev Simulation::calcJacobianAndSpeedsFromPrev src/simulation.cpp:546-608
+ *   d4_set_matrix        the CSC arrays Ap/Ai/Ax handed to UMFPACK  src/simulation.cpp:637-638
  *   d4_factor            calculateSparseFormForJacobian ->
  *                        umfpack_di_symbolic/numeric     src/simulation.cpp:635-640
  *   d4_solve             Simulation::solveEQSys -> umfpack_di_solve src/simulation.cpp:643-659
  *   d4_attempt           stages I-III + calculateXError   src/simulation.cpp:90-161,692-700
  *   d4_run               Simulation::run                  src/simulation.cpp:30-281
- *   d4_field_xy / d4_field_xy_diff_x  Field::xy / Field::xy_diff_x src/Fields/Field.cpp:295-346
+ *   d4_field_eval        Field::xy / Field::xy_diff_x    src/Fields/Field.cpp:333-346
  */
 #ifndef D4CORE_H
 #define D4CORE_H
@@ -147,13 +148,18 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
  * factor = (t_new - t_base) / (t_old - t_base); a_colmajor/dvec may be null. */
 int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *dvec);
 
+/* Replace the device matrix by a dense column-major n x n matrix (the
+ * umfpack_di_numeric input of src/simulation.cpp:638, expanded from CSC). */
+int d4_set_matrix(void *ctx, const double *a_colmajor);
+
 /* Factorise the device Jacobian.  Returns D4_WARN_SINGULAR on an exact zero
  * pivot, like umfpack_di_numeric. */
 int d4_factor(void *ctx);
 
 /* Solve A dx = g with the last factorisation (UMFPACK_A).  Returns
- * D4_WARN_SINGULAR like umfpack_di_solve; the caller zeroes entries outside
- * (-1, 1) as src/simulation.cpp:646-658 does (d4_attempt/d4_run do this). */
+ * D4_WARN_SINGULAR like umfpack_di_solve and, like it, leaves the result as
+ * computed; d4_attempt/d4_run apply solveEQSys's zeroing of entries outside
+ * (-1, 1) (src/simulation.cpp:646-658) themselves. */
 int d4_solve(void *ctx, const double *g, double *dx);
 
 /* Reset the per-dislocation tolerances (PrecisionHandler::reset). */
