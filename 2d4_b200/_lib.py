@@ -14,6 +14,7 @@ D4_ERR = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "ba
           -5: "I/O error"}
 D4_PREC_FP64, D4_PREC_MIXED = 0, 1
 D4_STRESS_NONE, D4_STRESS_FIXED_RATE, D4_STRESS_CYCLIC, D4_STRESS_INC_CYCLIC = 0, 1, 2, 3
+CATEGORIES = ["speeds", "jacobian", "factor", "solve", "rescale"]
 
 
 class Protocol(C.Structure):
@@ -78,6 +79,10 @@ SIGNATURES = {
     "d4_get_attempt": (C.c_int, [_vp, _dp, _dp, _dp]),
     "d4_run": (C.c_int, [_vp, C.POINTER(RunIO), C.POINTER(RunResult)]),
     "d4_field_eval": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp]),
+    "d4_advance": (C.c_int, [_vp, C.c_longlong, C.POINTER(RunResult)]),
+    "d4_profile": (C.c_int, [_vp, C.c_int]),
+    "d4_profile_read": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)]),
+    "d4_kernel_launches": (C.c_longlong, []),
 }
 
 _LIB = None

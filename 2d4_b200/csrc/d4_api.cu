@@ -10,6 +10,7 @@
 #include <cstring>
 #include <fstream>
 #include <iomanip>
+#include <algorithm>
 #include <new>
 #include <sstream>
 #include <string>
@@ -19,6 +20,42 @@
 
 using d4::Ctx;
 using d4::CudaError;
+
+namespace d4 {
+std::atomic<long long> g_launches{0};
+
+int prof_begin(Ctx &c, int cat) {
+    if (!c.prof.on) return -1;
+    if (c.prof.used * 2 + 2 > c.prof.pool.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            D4_CUDA_OK(cudaEventCreate(&e));
+            c.prof.pool.push_back(e);
+        }
+    }
+    const int idx = (int)c.prof.used++;
+    if ((size_t)idx >= c.prof.cat.size()) c.prof.cat.resize(idx + 1);
+    c.prof.cat[idx] = cat;
+    D4_CUDA_OK(cudaEventRecord(c.prof.pool[2 * idx], c.stream));
+    return idx;
+}
+
+void prof_end(Ctx &c, int idx) {
+    if (idx < 0) return;
+    cudaEventRecord(c.prof.pool[2 * idx + 1], c.stream);
+}
+
+void prof_collect(Ctx &c) {
+    for (size_t k = 0; k < c.prof.used; ++k) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c.prof.pool[2 * k], c.prof.pool[2 * k + 1]) == cudaSuccess) {
+            c.prof.ms[c.prof.cat[k]] += ms;
+            c.prof.calls[c.prof.cat[k]] += 1;
+        }
+    }
+    c.prof.used = 0;
+}
+}  // namespace d4
 
 namespace {
 
@@ -63,11 +100,13 @@ void dalloc(T **p, size_t count) {
 void free_all(Ctx *c) {
     void *bufs[] = {c->x0, c->y, c->xb, c->xh, c->x2, c->xs_tmp, c->ys_tmp, c->v_init,
                     c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
-                    c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red};
+                    c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red,
+                    c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_flags) cudaFreeHost(c->h_flags);
+    for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -83,6 +122,9 @@ int fail(Ctx *c, int code, const std::string &msg) {
     }                                                           \
     catch (const CudaError &e) {                                \
         return fail((c), D4_ERR_CUDA, e.what);                  \
+    }                                                           \
+    catch (const d4::StateError &e) {                           \
+        return fail((c), D4_ERR_STATE, e.what);                 \
     }                                                           \
     catch (const std::bad_alloc &) {                            \
         return fail((c), D4_ERR_NOMEM, "host allocation failed"); \
@@ -100,45 +142,68 @@ void sync(Ctx &c) { D4_CUDA_OK(cudaStreamSynchronize(c.stream)); }
 
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
+    using d4::ProfScope;
     const d4_protocol &pr = c.p.protocol;
     const double t_1__ = t0 + h;
     const double t_1p2 = t0 + h / 2;
-    int singular = 0, pivoted = 0, st;
+    int singular = 0, pivoted = 0;
+    auto jac = [&](const double *x, double hh, double ta, double tb, double *va, double *vb) {
+        ProfScope ps(c, D4_CAT_JACOBIAN);
+        d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
+    };
+    auto fac = [&]() {
+        int st;
+        {
+            ProfScope ps(c, D4_CAT_FACTOR);
+            st = d4::factor64(c);
+        }
+        singular |= st == D4_WARN_SINGULAR;
+        pivoted += c.factor_pivoted;
+    };
+    auto spd = [&](const double *x, double t, double *v) {
+        ProfScope ps(c, D4_CAT_SPEEDS);
+        d4::speeds64(c, x, c.y, ext_stress(pr, t), v);
+    };
+    auto slv = [&](int gmode, double hv, const double *se, const double *si, const double *xn,
+                   const double *xo, const double *base, double *out) {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update64(c, gmode, hv, se, si, xn, xo, base, out);
+    };
     // stage I: one large step
-    d4::jacobian64(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t_1__), c.v_init, c.speed);
-    st = d4::factor64(c);
-    singular |= st == D4_WARN_SINGULAR;
-    pivoted += c.factor_pivoted;
-    d4::solve_update64(c, d4::kGBig, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xb);
-    d4::speeds64(c, c.xb, c.y, ext_stress(pr, t_1__), c.speed2);
-    d4::solve_update64(c, d4::kGNewton, h, c.speed2, c.v_init, c.xb, c.x0, c.xb, c.xb);
+    jac(c.x0, h, t0, t_1__, c.v_init, c.speed);
+    fac();
+    slv(d4::kGBig, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xb);
+    spd(c.xb, t_1__, c.speed2);
+    slv(d4::kGNewton, h, c.speed2, c.v_init, c.xb, c.x0, c.xb, c.xb);
     // stage II: first small step, Jacobian from the previous one
     {
         const double factor = (t_1p2 - t0) / (t_1__ - t0);
-        d4::jacobian_from_prev64(c, factor);
-        st = d4::factor64(c);
-        singular |= st == D4_WARN_SINGULAR;
-        pivoted += c.factor_pivoted;
+        {
+            ProfScope ps(c, D4_CAT_RESCALE);
+            d4::jacobian_from_prev64(c, factor);
+        }
+        fac();
         const double dif = ext_stress(pr, t_1p2) - ext_stress(pr, t_1__);
         d4::shift_speed64(c, c.speed, dif);
     }
-    d4::solve_update64(c, d4::kGHalf, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xh);
-    d4::speeds64(c, c.xh, c.y, ext_stress(pr, t_1p2), c.speed2);
-    d4::solve_update64(c, d4::kGNewton, h / 2, c.speed2, c.v_init, c.xh, c.x0, c.xh, c.xh);
+    slv(d4::kGHalf, h, c.speed, c.v_init, nullptr, nullptr, c.x0, c.xh);
+    spd(c.xh, t_1p2, c.speed2);
+    slv(d4::kGNewton, h / 2, c.speed2, c.v_init, c.xh, c.x0, c.xh, c.xh);
     // stage III: second small step
-    d4::jacobian64(c, c.xh, c.y, h / 2, ext_stress(pr, t_1p2), ext_stress(pr, t_1__), c.v_init2,
-                   c.speed2);
-    st = d4::factor64(c);
-    singular |= st == D4_WARN_SINGULAR;
-    pivoted += c.factor_pivoted;
-    d4::solve_update64(c, d4::kGHalf, h, c.speed2, c.v_init2, nullptr, nullptr, c.xh, c.x2);
-    d4::speeds64(c, c.x2, c.y, ext_stress(pr, t_1__), c.speed2);
-    d4::solve_update64(c, d4::kGNewton, h / 2, c.speed2, c.v_init2, c.x2, c.xh, c.x2, c.x2);
+    jac(c.xh, h / 2, t_1p2, t_1__, c.v_init2, c.speed2);
+    fac();
+    slv(d4::kGHalf, h, c.speed2, c.v_init2, nullptr, nullptr, c.xh, c.x2);
+    spd(c.x2, t_1__, c.speed2);
+    slv(d4::kGNewton, h / 2, c.speed2, c.v_init2, c.x2, c.xh, c.x2, c.x2);
     // stage IV: error ratio
     d4::error_ratio64(c, c.xb, c.x2);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost,
                                c.stream));
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags + 7, c.wave_err, sizeof(int), cudaMemcpyDeviceToHost,
+                               c.stream));
     sync(c);
+    if (c.prof.on) d4::prof_collect(c);
+    if (c.h_flags[7]) throw d4::StateError("triangular solve wavefront timed out");
     const int idx = (int)c.h_red[1];
     if (idx >= 0) c.selected_id = idx;
     res->ratio = c.h_red[0] / c.dipole_prec_sq;
@@ -247,6 +312,15 @@ int d4_create(void **out, int n, const d4_params *p) {
         dalloc(&c->perm, (size_t)n);
         dalloc(&c->flags, (size_t)d4::kFlagCount);
         dalloc(&c->red, 8);
+        const int nblk = (n + 31) / 32;
+        dalloc(&c->wave_done, (size_t)nblk);
+        dalloc(&c->wave_done2, (size_t)nblk);
+        dalloc(&c->wave_err, 1);
+        dalloc(&c->xw1, (size_t)n);
+        dalloc(&c->xw2, (size_t)n);
+        D4_CUDA_OK(cudaMemset(c->wave_done, 0, sizeof(unsigned) * nblk));
+        D4_CUDA_OK(cudaMemset(c->wave_done2, 0, sizeof(unsigned) * nblk));
+        D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int)));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_red, sizeof(double) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_flags, sizeof(int) * d4::kFlagCount));
         D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
@@ -441,72 +515,45 @@ int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, doub
     D4_GUARD_END(c)
 }
 
-// Simulation::run, src/simulation.cpp:30-281.
-int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
-    Ctx *c = (Ctx *)ctx;
-    if (!c) return D4_ERR_ARG;
-    D4_GUARD_BEGIN
+// One pass of Simulation::run's loop body per attempt (src/simulation.cpp:88-277),
+// until `target` accepted steps (target < 0: until interrupt()).
+static int run_loop(Ctx *c, const d4_run_io *io, std::ofstream *log, long long target) {
     const d4_params &p = c->p;
     const int n = c->n;
-    d4_run_io none{};
-    if (!io) io = &none;
-    std::ofstream log;
-    if (io->log_path && *io->log_path) {
-        log.open(io->log_path);
-        if (!log) return fail(c, D4_ERR_IO, std::string("cannot open log ") + io->log_path);
-        log << std::scientific << std::setprecision(16);
-    }
-    const bool want_log = log.is_open();
+    d4::RunState &rs = c->rs;
+    const bool want_log = log && log->is_open();
     std::vector<double> hv(n), hv2(n), hv3(n);
-    double strain = 0, energy = 0, h_before_writeout = 0;
-    long long ok = 0, failed = 0, attempts = 0, n_piv = 0, n_sing = 0;
-    long long aval_count = 0;
-    bool in_aval = false;
-    unsigned sub_counter = 0;
-    double next_wo = p.save_sub_configs ? next_write_out(p, c->sim_time) : INFINITY;
     double *d_strain = c->red + 4;
-
-    D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
-    // src/simulation.cpp:46: initial speeds (also seeds the tolerances)
-    d4::speeds64(*c, c->x0, c->y, ext_stress(p.protocol, c->sim_time), c->v_init);
-    if (want_log) {
-        download(*c, hv.data(), c->v_init);
-        sync(*c);
-        const double sum_avg = host_abs_sum(hv) / n;
-        log << "# simTime(1)\tsuccessfullSteps(2)\tfailedSteps(3)\tmaxErrorRatioSqr(4)\t"
-               "maxErrorRatioID(5)\tsumAvgSp(6)\tcutOff(7)\torderParameter(8)\t"
-               "externalStress(9)\ttimeStageI - III(10)\tstrain(11)\tvSquare(12)\t"
-               "energy(13)\twallTimeElapsed(14)\tstepSize(15)\t\n";
-        log << c->sim_time << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t" << sum_avg
-            << "\t" << c->cutoff << "\t-\t" << ext_stress(p.protocol, c->sim_time) << "\t-\t"
-            << strain << "\t" << host_sq_sum(hv) << "\t" << energy << "\t" << 0 << "\t"
-            << c->step_size << "\n";
-    }
+    const long long ok_start = rs.ok;
     for (;;) {
-        // interrupt(), src/simulation.cpp:722-750
-        if (p.time_limit >= 0 && c->sim_time > p.time_limit) break;
-        if (p.strain_increase_limit >= 0 && strain > p.strain_increase_limit) break;
-        if (p.step_count_limit >= 0 && ok > p.step_count_limit) break;
-        if (p.avalanche_limit >= 0 && aval_count > p.avalanche_limit) break;
-        if (io->max_attempts > 0 && attempts >= io->max_attempts) break;
+        if (target >= 0) {
+            if (rs.ok - ok_start >= target) break;
+        } else {
+            // interrupt(), src/simulation.cpp:722-750
+            if (p.time_limit >= 0 && c->sim_time > p.time_limit) break;
+            if (p.strain_increase_limit >= 0 && rs.strain > p.strain_increase_limit) break;
+            if (p.step_count_limit >= 0 && rs.ok > p.step_count_limit) break;
+            if (p.avalanche_limit >= 0 && rs.aval_count > p.avalanche_limit) break;
+        }
+        if (io && io->max_attempts > 0 && rs.attempts >= io->max_attempts) break;
 
         const double h = c->step_size;
         d4_attempt_result ar;
         attempt(*c, c->sim_time, h, &ar);
-        ++attempts;
-        n_piv += ar.pivoted;
-        n_sing += ar.singular;
+        ++rs.attempts;
+        rs.pivoted += ar.pivoted;
+        rs.singular += ar.singular;
         if (ar.ratio < 1) {
             c->sim_time += h;
-            ++ok;
+            ++rs.ok;
             if (p.calculate_strain) {
                 d4::strain_increment64(*c, c->x0, c->xh, d_strain);
                 d4::strain_increment64(*c, c->xh, c->x2, d_strain + 1);
                 D4_CUDA_OK(cudaMemcpyAsync(c->h_red + 4, d_strain, sizeof(double) * 2,
                                            cudaMemcpyDeviceToHost, c->stream));
                 sync(*c);
-                strain += c->h_red[4];
-                strain += c->h_red[5];
+                rs.strain += c->h_red[4];
+                rs.strain += c->h_red[5];
             }
             d4::normalize64(*c, c->x0, c->x2);
             const bool need_speed = want_log || p.avalanche_limit >= 0;
@@ -521,83 +568,177 @@ int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
                 download(*c, hv3.data(), c->speed2);
                 sync(*c);
                 const double vsq_end = host_sq_sum(hv3);
-                energy += (host_sq_sum(hv) + 2 * host_sq_sum(hv2) + vsq_end) * h / 4;
-                log << c->sim_time << "\t" << ok << "\t" << failed << "\t" << ar.ratio << "\t"
-                    << ar.max_id << "\t" << sum_avg << "\t" << c->cutoff << "\t";
+                rs.energy += (host_sq_sum(hv) + 2 * host_sq_sum(hv2) + vsq_end) * h / 4;
+                *log << c->sim_time << "\t" << rs.ok << "\t" << rs.failed << "\t" << ar.ratio
+                     << "\t" << ar.max_id << "\t" << sum_avg << "\t" << c->cutoff << "\t";
                 if (p.calculate_order_parameter) {
                     download(*c, hv3.data(), c->speed);
                     sync(*c);
                     double op = 0;
                     for (int i = 0; i < n; ++i) op += (i < n / 2 ? 1 : -1) * hv3[i];
-                    log << op << "\t";
+                    *log << op << "\t";
                 } else
-                    log << "-\t";
-                log << ext_stress(p.protocol, c->sim_time) << "\t" << 0 << "\t";
+                    *log << "-\t";
+                *log << ext_stress(p.protocol, c->sim_time) << "\t" << 0 << "\t";
                 if (p.calculate_strain)
-                    log << strain << "\t";
+                    *log << rs.strain << "\t";
                 else
-                    log << "-\t";
-                log << vsq_end << "\t" << energy << "\t" << 0 << "\t" << h << "\n";
+                    *log << "-\t";
+                *log << vsq_end << "\t" << rs.energy << "\t" << 0 << "\t" << h << "\n";
             }
             if (p.avalanche_limit >= 0) {
-                if (in_aval && sum_avg < p.avalanche_speed_threshold) {
-                    ++aval_count;
-                    in_aval = false;
+                if (rs.in_aval && sum_avg < p.avalanche_speed_threshold) {
+                    ++rs.aval_count;
+                    rs.in_aval = false;
                 } else if (sum_avg > p.avalanche_speed_threshold)
-                    in_aval = true;
+                    rs.in_aval = true;
             }
             if (p.save_sub_configs) {
-                if ((!in_aval && p.sub_config_delay <= sub_counter) ||
-                    (in_aval && p.sub_config_delay_during_avalanche <= sub_counter) ||
-                    next_wo <= c->sim_time) {
-                    sub_counter = 0;
-                    next_wo = next_write_out(p, c->sim_time);
-                    if (io->sub_config_prefix) {
+                if ((!rs.in_aval && p.sub_config_delay <= rs.sub_counter) ||
+                    (rs.in_aval && p.sub_config_delay_during_avalanche <= rs.sub_counter) ||
+                    rs.next_wo <= c->sim_time) {
+                    rs.sub_counter = 0;
+                    rs.next_wo = next_write_out(p, c->sim_time);
+                    if (io && io->sub_config_prefix) {
                         std::stringstream ss;
                         ss << std::setprecision(9) << c->sim_time;
                         write_config(*c, std::string(io->sub_config_prefix) + ss.str() + ".dconf",
                                      io->order);
                     }
                 } else
-                    ++sub_counter;
+                    ++rs.sub_counter;
             }
         } else
-            ++failed;
+            ++rs.failed;
         // PrecisionHandler::getNewStepSize (src/precision_handler.cpp:57-62) and
         // the write-out clipping of src/simulation.cpp:253-274
         double hn = 0.9 * h * std::min(2., std::pow(ar.ratio, -1. / 6));
-        if (h_before_writeout != 0) {
-            if (ar.ratio < 1) hn = std::max(hn, h_before_writeout);
-            h_before_writeout = 0;
+        if (rs.h_before_writeout != 0) {
+            if (ar.ratio < 1) hn = std::max(hn, rs.h_before_writeout);
+            rs.h_before_writeout = 0;
         }
-        const double rem = std::nextafter(next_wo, INFINITY) - c->sim_time;
+        const double rem = std::nextafter(rs.next_wo, INFINITY) - c->sim_time;
         if (rem < hn) {
-            h_before_writeout = hn;
+            rs.h_before_writeout = hn;
             hn = rem;
         }
         if (c->use_dipole) d4::reset_tol64(*c);
         if (p.max_stepsize > 0 && p.max_stepsize < hn) hn = p.max_stepsize;
         c->step_size = hn;
     }
+    return D4_OK;
+}
+
+static void fill_result(Ctx *c, const d4::RunState &before, float ms, d4_run_result *res) {
+    if (!res) return;
+    const d4::RunState &rs = c->rs;
+    res->sim_time = c->sim_time;
+    res->step_size = c->step_size;
+    res->strain = rs.strain - before.strain;
+    res->energy = rs.energy - before.energy;
+    res->successful_steps = rs.ok - before.ok;
+    res->failed_steps = rs.failed - before.failed;
+    res->attempts = rs.attempts - before.attempts;
+    res->pivoted_factorizations = rs.pivoted - before.pivoted;
+    res->singular_factorizations = rs.singular - before.singular;
+    res->device_seconds = ms / 1000.0;
+}
+
+static void start_state(Ctx *c) {
+    c->rs = d4::RunState();
+    c->rs.started = true;
+    c->rs.next_wo = c->p.save_sub_configs ? next_write_out(c->p, c->sim_time) : INFINITY;
+}
+
+// Simulation::run, src/simulation.cpp:30-281.
+int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    const d4_params &p = c->p;
+    const int n = c->n;
+    std::ofstream log;
+    if (io && io->log_path && *io->log_path) {
+        log.open(io->log_path);
+        if (!log) return fail(c, D4_ERR_IO, std::string("cannot open log ") + io->log_path);
+        log << std::scientific << std::setprecision(16);
+    }
+    start_state(c);
+    const d4::RunState before = c->rs;
+    D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
+    // src/simulation.cpp:46: initial speeds (also seeds the tolerances)
+    d4::speeds64(*c, c->x0, c->y, ext_stress(p.protocol, c->sim_time), c->v_init);
+    if (log.is_open()) {
+        std::vector<double> hv(n);
+        download(*c, hv.data(), c->v_init);
+        sync(*c);
+        log << "# simTime(1)\tsuccessfullSteps(2)\tfailedSteps(3)\tmaxErrorRatioSqr(4)\t"
+               "maxErrorRatioID(5)\tsumAvgSp(6)\tcutOff(7)\torderParameter(8)\t"
+               "externalStress(9)\ttimeStageI - III(10)\tstrain(11)\tvSquare(12)\t"
+               "energy(13)\twallTimeElapsed(14)\tstepSize(15)\t\n";
+        log << c->sim_time << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t" << 0 << "\t"
+            << host_abs_sum(hv) / n << "\t" << c->cutoff << "\t-\t"
+            << ext_stress(p.protocol, c->sim_time) << "\t-\t" << 0.0 << "\t" << host_sq_sum(hv)
+            << "\t" << 0.0 << "\t" << 0 << "\t" << c->step_size << "\n";
+    }
+    run_loop(c, io, &log, -1);
     D4_CUDA_OK(cudaEventRecord(c->ev1, c->stream));
     sync(*c);
     float ms = 0;
     D4_CUDA_OK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    if (io->end_config_path) write_config(*c, io->end_config_path, io->order);
-    if (res) {
-        res->sim_time = c->sim_time;
-        res->step_size = c->step_size;
-        res->strain = strain;
-        res->energy = energy;
-        res->successful_steps = ok;
-        res->failed_steps = failed;
-        res->attempts = attempts;
-        res->pivoted_factorizations = n_piv;
-        res->singular_factorizations = n_sing;
-        res->device_seconds = ms / 1000.0;
+    if (io && io->end_config_path) write_config(*c, io->end_config_path, io->order);
+    fill_result(c, before, ms, res);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_advance(void *ctx, long long accepted_steps, d4_run_result *res) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || accepted_steps < 0) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    if (!c->rs.started) {
+        start_state(c);
+        // the first attempt's tolerances include the initial sweep of run()
+        d4::speeds64(*c, c->x0, c->y, ext_stress(c->p.protocol, c->sim_time), c->v_init);
+    }
+    const d4::RunState before = c->rs;
+    D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
+    run_loop(c, nullptr, nullptr, accepted_steps);
+    D4_CUDA_OK(cudaEventRecord(c->ev1, c->stream));
+    sync(*c);
+    float ms = 0;
+    D4_CUDA_OK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    fill_result(c, before, ms, res);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_profile(void *ctx, int enable) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    c->prof.on = enable != 0;
+    c->prof.used = 0;
+    for (int k = 0; k < D4_CAT_COUNT; ++k) {
+        c->prof.ms[k] = 0;
+        c->prof.calls[k] = 0;
+    }
+    return D4_OK;
+}
+
+int d4_profile_read(void *ctx, double *ms, long long *calls) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !ms || !calls) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    sync(*c);
+    d4::prof_collect(*c);
+    for (int k = 0; k < D4_CAT_COUNT; ++k) {
+        ms[k] = c->prof.ms[k];
+        calls[k] = c->prof.calls[k];
     }
     return D4_OK;
     D4_GUARD_END(c)
 }
+
+long long d4_kernel_launches(void) { return d4::g_launches.load(); }
 
 }  // extern "C"

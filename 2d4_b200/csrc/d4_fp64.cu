@@ -121,12 +121,22 @@ __global__ void __launch_bounds__(256) k_pairs64(PairArgs a) {
 }
 
 // Ordered row sums of the stress sweep: v_i = sum_j F[i, j] + ext * b_i.
+// Loads are issued 8 at a time ahead of the (sequential, ordered) additions.
 __global__ void k_rows_speed64(int n, const double *__restrict__ F, double ext, double *v) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0;
     const double *col = F + i;
-    for (int j = 0; j < n; ++j)
+    int j = 0;
+    for (; j + 8 <= n; j += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t[u] = __ldg(col + (size_t)(j + u) * n);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (j + u != i) s += t[u];
+    }
+    for (; j < n; ++j)
         if (j != i) s += col[(size_t)j * n];
     v[i] = s + ext * bsign(i, n);
 }
@@ -139,7 +149,22 @@ __global__ void k_rows_jac64(int n, const double *__restrict__ F, double *A, dou
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0, sub = 0;
-    for (int j = 0; j < n; ++j) {
+    int j = 0;
+    for (; j + 8 <= n; j += 8) {
+        double tf[8], ta[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            tf[u] = __ldg(F + (size_t)i + (size_t)(j + u) * n);
+            ta[u] = A[(size_t)i + (size_t)(j + u) * n];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (j + u != i) {
+                s += tf[u];
+                sub -= ta[u];
+            }
+    }
+    for (; j < n; ++j) {
         if (j == i) continue;
         s += F[(size_t)i + (size_t)j * n];
         sub -= A[(size_t)i + (size_t)j * n];
@@ -150,7 +175,7 @@ __global__ void k_rows_jac64(int n, const double *__restrict__ F, double *A, dou
     const double d = f64::weight(sub, wfn);
     dvec[i] = d;
     const double sc = (1 + d) / 2;
-    for (int j = 0; j < n; ++j) {
+    for (j = 0; j < n; ++j) {
         double *e = A + (size_t)i + (size_t)j * n;
         if (j == i)
             *e = sub * sc + 1;

@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
+#include <vector>
 
 #include "d4core.h"
 
@@ -20,6 +22,25 @@ enum FlagSlot {
     kFlagNeedPivot = 0,  // fast LU met |a_ik| > |a_kk| or a_kk == 0: partial pivoting would swap
     kFlagSingular = 1,   // pivoted LU met an exact zero pivot
     kFlagCount = 8
+};
+
+// State of Simulation::run's loop kept between d4_advance calls.
+struct RunState {
+    bool started = false;
+    double strain = 0, energy = 0, h_before_writeout = 0, next_wo = 0;
+    long long ok = 0, failed = 0, attempts = 0, pivoted = 0, singular = 0;
+    long long aval_count = 0;
+    bool in_aval = false;
+    unsigned sub_counter = 0;
+};
+
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;      // pairs (start, stop)
+    std::vector<int> cat;               // category per pair in use
+    size_t used = 0;
+    double ms[D4_CAT_COUNT] = {};
+    long long calls[D4_CAT_COUNT] = {};
 };
 
 struct Ctx {
@@ -55,7 +76,31 @@ struct Ctx {
     // pinned host mirror of the small results
     double *h_red = nullptr;
     int *h_flags = nullptr;
+
+    // wavefront triangular solves: per-block done flags (epoch-tagged),
+    // intermediate vectors and the spin-limit error flag
+    unsigned *wave_done = nullptr, *wave_done2 = nullptr;
+    unsigned wave_epoch = 0;
+    int *wave_err = nullptr;
+    double *xw1 = nullptr, *xw2 = nullptr;
+
+    RunState rs;
+    Prof prof;
 };
+
+// Category timing: returns the index of an event pair (or -1 when off).
+int prof_begin(Ctx &c, int cat);
+void prof_end(Ctx &c, int idx);
+void prof_collect(Ctx &c);  // after a stream sync: folds finished pairs into totals
+
+struct ProfScope {
+    Ctx &c;
+    int idx;
+    ProfScope(Ctx &cc, int cat) : c(cc), idx(prof_begin(cc, cat)) {}
+    ~ProfScope() { prof_end(c, idx); }
+};
+
+extern std::atomic<long long> g_launches;
 
 // ---- FP64 pair sweeps (d4_fp64.cu) ----
 // Stress sweep: F (signed pair forces) and tolerance update, then ordered row sums.
@@ -101,7 +146,12 @@ struct CudaError {
           what(std::string(cudaGetErrorString(c)) + " at " + file + ":" + std::to_string(line) +
                " (" + expr + ")") {}
 };
+struct StateError {
+    std::string what;
+    explicit StateError(const char *w) : what(w) {}
+};
 inline void check_launch(const char *name) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw CudaError(e, name, __FILE__, __LINE__);
 }

@@ -252,6 +252,22 @@ class Engine:
         self._call("d4_get_attempt", _lib.ptr(xb), _lib.ptr(xh), _lib.ptr(x2))
         return r, xb, xh, x2
 
+    def advance(self, accepted_steps):
+        """Continues the stepping loop for exactly `accepted_steps` accepted steps."""
+        r = _lib.RunResult()
+        self._call("d4_advance", C.c_longlong(accepted_steps), C.byref(r))
+        return r
+
+    def profile(self, enable=True):
+        self._call("d4_profile", int(bool(enable)))
+
+    def profile_read(self):
+        ms = np.zeros(len(_lib.CATEGORIES))
+        calls = np.zeros(len(_lib.CATEGORIES), dtype=np.int64)
+        self._call("d4_profile_read", _lib.ptr(ms),
+                   calls.ctypes.data_as(C.POINTER(C.c_longlong)))
+        return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(_lib.CATEGORIES)}
+
     def positions(self):
         x = np.empty(self.n)
         y = np.empty(self.n)

@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Throughput of the 2D4_sim implicit step on B200: dislocation-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c3-fp64] [--no-cpu-baseline]
+
+A step is one ACCEPTED implicit step (stages I-IV of src/simulation.cpp:88-277;
+the failed attempts between accepted steps are part of its cost).  The metric is
+dislocation-steps/s = N x accepted steps / seconds.
+
+Default workload (c2): N=1024 dislocations (512 +b / 512 -b), dense N x N
+Jacobian, no cutoff, plain FP64 form; starting from the N=1024 configuration
+(seed 1001, iid uniform) relaxed for 500 accepted steps at zero stress by the
+reference itself (tests/golden/c2_relaxed_1024.npz), then constant external
+stress tau = 0.05 (FixedRateProtocol(0.05, 0)) with time and step size reset,
+default precision (-P 1e-5 -p 0.05).  Synthetic seeded data; no dataset.
+
+Timing: W warm-up steps, then K steps, each timed on the device with CUDA
+events around one d4_advance(1) call on the library's stream, with a 512 MiB
+buffer written between steps to flush L2 (the step's working set, ~24 MB, is
+below L2).  Multi-GPU (--gpus N under torchrun): the single system does not
+shard (one GPU per system), so each rank runs an independent replica (weak
+scaling); the time is the max over ranks and value = total steps of all ranks x
+N / that time.
+
+--impl reference: the reference core built from its own sources with its own
+flags (oracle/_ref/libd4ref_fast.so, UMFPACK replaced by OpenBLAS dgetrf/dgetrs on
+all host cores) on the same workload, through Simulation::run, rank 0 only.
+"""
+import argparse
+import glob
+import importlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic work per unit (frozen; counted from the kernel sources, see
+# DESIGN.md): FLOP per unique pair of a stress sweep and of a fused
+# stress + gradient sweep, and the LU/solve counts of a dense N x N system.
+W_STRESS_PAIR = 136
+W_FUSED_PAIR = 386
+
+WORKLOADS = {
+    "c2": dict(n=1024, tau=0.05, precision=1e-5, source="relaxed",
+               desc="N=1024 plain FP64, dense Jacobian, relaxed 500 steps, then tau_ext=0.05"),
+    "c1": dict(n=64, tau=0.0, precision=1e-8, source=("seed", 1000),
+               desc="N=64 plain FP64, tau_ext=0, P=1e-8"),
+    "c3-fp64": dict(n=4096, tau=0.1, precision=1e-5, source=("seed", 1002),
+                    desc="N=4096 plain FP64, dense Jacobian, tau_ext=0.1"),
+}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def start_state(pkg, wl):
+    n = wl["n"]
+    if wl["source"] == "relaxed":
+        z = np.load(os.path.join(ROOT, "tests", "golden", "c2_relaxed_1024.npz"))
+        return z["x"].copy(), z["y"].copy()
+    x, y, _ = pkg.dconf.generate_internal(n, wl["source"][1])
+    return x, y
+
+
+def make_sd(pkg, x, y, wl):
+    sd = pkg.SimulationData()
+    sd.set_positions(x, y)
+    sd.precision = wl["precision"]
+    sd.external_stress = pkg.FixedRateProtocol(wl["tau"], 0.0)
+    return sd
+
+
+def openblas_path():
+    try:
+        import scipy
+        libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs",
+                                      "libscipy_openblas-*.so"))
+        return libs[0] if libs else None
+    except Exception:
+        return None
+
+
+def reference_run(wl, x, y, steps, warmup=0):
+    """Times the reference core (oracle/_ref, reference flags) on the workload:
+    `steps` accepted steps after a `warmup`-step run from the same state."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    ob = openblas_path()
+    if ob:
+        os.environ["D4REF_OPENBLAS"] = ob
+        os.environ.setdefault("D4REF_THREADS", str(os.cpu_count() or 1))
+    import pyoracle  # the CPU baseline leg: reference build, timed, never the product
+    pkg = importlib.import_module("2d4_b200")
+    ref = pyoracle.Reference("fast")
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "start.dconf")
+    b = np.where(np.arange(len(x)) < len(x) // 2, 1, -1)
+    pkg.dconf.write(path, x, y, b, digits=17)
+    kw = dict(position_precision=wl["precision"], const_external_stress=wl["tau"], has_rate=1,
+              rate=0.0)
+    if warmup > 0:
+        ref.run(path, ref.params(step_count_limit=warmup - 1, **kw))
+    xr, yr, res, wall = ref.run(path, ref.params(step_count_limit=steps - 1, **kw))
+    return dict(steps=int(res.successful_steps), failed=int(res.failed_steps), wall=wall,
+                value=wl["n"] * res.successful_steps / wall,
+                cores=int(os.environ.get("D4REF_THREADS", "1")) if ob else 1,
+                solver="OpenBLAS dgetrf/dgetrs" if ob else "shim LU (1 thread)")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([t.strip() for t in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def fp64_peak_tflops(torch, device):
+    """cuBLAS DGEMM 4096^3 (2 N^3 FLOP), best of 5: the FP64 roofline."""
+    a = torch.randn(4096, 4096, dtype=torch.float64, device=device)
+    b = torch.randn(4096, 4096, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    return 2 * 4096 ** 3 / best / 1e12
+
+
+def roofline(prof, n, hbm_gbs, fp64_tf):
+    """Roofline of the dominant kernel category of the timed region."""
+    cat = max(prof, key=lambda k: prof[k][0])
+    ms, calls = prof[cat]
+    per = ms / max(calls, 1) / 1e3  # seconds per call
+    pairs = n * (n - 1) / 2
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("%s_n%d" % (cat, n))
+    if cat == "solve":
+        algo = 8.0 * n * n + 7 * 8.0 * n  # L and U read once, vectors
+        ach = algo / per / 1e9
+        return dict(kernel=cat, bound="hbm", achieved=ach, peak=hbm_gbs, unit="GB/s",
+                    frac=ach / hbm_gbs, traffic=traffic, algorithmic_per_launch=algo,
+                    launch_ms=per * 1e3, share=ms / sum(v[0] for v in prof.values()))
+    if cat == "factor":
+        algo = 2.0 / 3.0 * n ** 3
+    elif cat == "jacobian":
+        algo = pairs * W_FUSED_PAIR
+    elif cat == "speeds":
+        algo = pairs * W_STRESS_PAIR
+    else:
+        algo = 16.0 * n * n
+    ach = algo / per / 1e12
+    return dict(kernel=cat, bound="tensor", achieved=ach, peak=fp64_tf, unit="TFLOP/s",
+                frac=ach / fp64_tf, traffic=traffic, algorithmic_per_launch=algo,
+                launch_ms=per * 1e3, share=ms / sum(v[0] for v in prof.values()),
+                peak_source="cuBLAS DGEMM 4096^3 measured in this run (FP64 peak)")
+
+
+def run_reference_arm(args, wl):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    try:
+        pkg = importlib.import_module("2d4_b200")
+        x, y = start_state(pkg, wl)
+        # bounded: about 2 minutes of CPU work at most
+        per_step = {64: 0.002, 1024: 0.5, 4096: 25.0}.get(wl["n"], 1.0)
+        k = max(2, min(args.steps, int(120 / per_step)))
+        r = reference_run(wl, x, y, k, warmup=min(args.warmup, 2))
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle failed: %s" % e}))
+        return
+    ms = 1e3 * r["wall"] / max(r["steps"], 1)
+    line = {"impl": "reference", "metric": "dislocation-steps/s", "value": r["value"],
+            "unit": "dislocation-steps/s", "n_gpus": args.gpus, "steps": r["steps"],
+            "warmup": min(args.warmup, 2), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["desc"], "n": wl["n"], "failed_steps": r["failed"]},
+            "cpu_baseline": {"value": r["value"], "unit": "dislocation-steps/s",
+                             "cores": r["cores"], "kind": "reference",
+                             "sample": "%d accepted steps of the same workload (reference "
+                                       "core, -Ofast build, %s)" % (r["steps"], r["solver"])},
+            "e2e": {"value": r["value"], "unit": "dislocation-steps/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import torch
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    pkg = importlib.import_module("2d4_b200")
+    lib = pkg._lib.load()
+    n = wl["n"]
+    x, y = start_state(pkg, wl)
+    eng = pkg.Engine(make_sd(pkg, x, y, wl), device=local)
+    for _ in range(args.warmup):
+        eng.advance(1)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    launches0 = lib.d4_kernel_launches()
+    eng.profile(True)
+    clocks.start()
+    barrier()
+    t_dev, attempts, failed = 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r = eng.advance(1)
+        t_dev += r.device_seconds
+        attempts += r.attempts
+        failed += r.failed_steps
+    barrier()
+    clk = clocks.stop()
+    launches = lib.d4_kernel_launches() - launches0
+    prof = eng.profile_read()
+    eng.profile(False)
+
+    # end to end through the public API: host positions in, step, host positions out
+    xh = np.empty(n)
+    yh = np.empty(n)
+    eng_x, eng_y = eng.positions()
+    xh[:] = eng_x
+    yh[:] = eng_y
+    pin_x = torch.from_numpy(xh).pin_memory().numpy()
+    pin_y = torch.from_numpy(yh).pin_memory().numpy()
+    barrier()
+    t_e2e = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng._call("d4_set_positions", pkg._lib.ptr(pin_x), pkg._lib.ptr(pin_y))
+        eng.advance(1)
+        eng._call("d4_get_positions", pkg._lib.ptr(pin_x), pkg._lib.ptr(pin_y))
+        t_e2e += time.perf_counter() - t0
+    barrier()
+
+    t_max, e2e_max = t_dev, t_e2e
+    if dist:
+        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max, e2e_max = float(tt[0]), float(tt[1])
+    total_steps = args.steps * ws
+    value = n * total_steps / t_max
+    e2e = n * total_steps / e2e_max
+    if rank != 0:
+        eng.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+    hbm, bf16, peak_src = measured_peaks()
+    fp64_tf = fp64_peak_tflops(torch, device)
+    roof = roofline(prof, n, hbm, fp64_tf)
+    roof["hbm_peak_source"] = peak_src
+    line = {"metric": "dislocation-steps/s", "value": value, "unit": "dislocation-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["desc"], "n": n, "form": "plain FP64",
+                       "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "flushed between steps (512 MiB write)",
+                       "attempts": attempts, "failed_steps": failed},
+            "e2e": {"value": e2e, "unit": "dislocation-steps/s",
+                    "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
+            "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
+            "kernel_ms": {k: v[0] for k, v in prof.items()},
+            "kernel_calls": {k: v[1] for k, v in prof.items()}}
+    if ws == 1 and not args.no_cpu_baseline:
+        try:
+            per_step = {64: 0.002, 1024: 0.5, 4096: 25.0}.get(n, 1.0)
+            k = max(2, min(20, int(15 / per_step)))
+            cb = reference_run(wl, x, y, k)
+            line["cpu_baseline"] = {"value": cb["value"], "unit": "dislocation-steps/s",
+                                    "cores": cb["cores"], "kind": "reference",
+                                    "sample": "%d accepted steps of the same workload from the "
+                                              "same start (reference core, -Ofast build, %s)"
+                                              % (cb["steps"], cb["solver"])}
+        except Exception as e:  # pragma: no cover
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

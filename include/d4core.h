@@ -24,6 +24,7 @@
  *   d4_solve             Simulation::solveEQSys -> umfpack_di_solve src/simulation.cpp:643-659
  *   d4_attempt           stages I-III + calculateXError   src/simulation.cpp:90-161,692-700
  *   d4_run               Simulation::run                  src/simulation.cpp:30-281
+ *   d4_advance           the body of Simulation::run's loop  src/simulation.cpp:88-277
  *   d4_field_eval        Field::xy / Field::xy_diff_x    src/Fields/Field.cpp:333-346
  */
 #ifndef D4CORE_H
@@ -172,6 +173,25 @@ int d4_get_attempt(void *ctx, double *x_big, double *x_half, double *x_two);
 
 /* Simulation::run on the context's positions; positions are updated. */
 int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res);
+
+/* Continue the stepping loop of d4_run for exactly `accepted_steps` accepted
+ * steps (failed attempts in between included), keeping the loop state (time,
+ * step size, write-out suggestion, counters) in the context between calls.  No
+ * initial sweep and no log.  res (may be null) gets the totals of this call,
+ * device_seconds the CUDA-event span of the call on the context's stream. */
+int d4_advance(void *ctx, long long accepted_steps, d4_run_result *res);
+
+/* Per-category device timing of the hot kernels (CUDA events on the context's
+ * stream).  Categories: 0 stress sweep, 1 fused Jacobian sweep, 2 factorisation,
+ * 3 solve, 4 half-step rescale.  d4_profile(ctx, 1) clears and starts; the
+ * totals (milliseconds) and call counts accumulate until read. */
+enum { D4_CAT_SPEEDS = 0, D4_CAT_JACOBIAN = 1, D4_CAT_FACTOR = 2, D4_CAT_SOLVE = 3,
+       D4_CAT_RESCALE = 4, D4_CAT_COUNT = 5 };
+int d4_profile(void *ctx, int enable);
+int d4_profile_read(void *ctx, double *ms, long long *calls);
+
+/* Number of kernels this library has launched in the process so far. */
+long long d4_kernel_launches(void);
 
 /* Single field evaluations on the device (FP64 path), for checks. */
 int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
