@@ -83,6 +83,8 @@ SIGNATURES = {
     "d4_profile": (C.c_int, [_vp, C.c_int]),
     "d4_profile_read": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)]),
     "d4_kernel_launches": (C.c_longlong, []),
+    "d4_speeds_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                    C.c_void_p, C.c_double, C.c_void_p]),
 }
 
 _LIB = None

@@ -14,6 +14,7 @@
 // (PrecisionHandler::updateTolerance) is a min, reduced with 64-bit atomicMin on
 // the bit pattern of the non-negative distance.
 #include <cstdint>
+#include <mutex>
 
 #include "d4_field64.cuh"
 #include "d4_internal.h"
@@ -384,3 +385,71 @@ void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double 
 }
 
 }  // namespace d4
+
+// ---------------------------------------------------------------------------
+// Allocation-free stress sweep.
+//
+// Some callers cannot allocate device memory at all: code that runs while a
+// stream is being captured into a CUDA graph (an allocation there breaks the
+// capture), real-time stepping loops that must not block on the allocator,
+// and hosts whose device memory is owned by another framework's allocator
+// that this library must not bypass.  For them, d4_speeds_noalloc runs the
+// FP64 stress sweep with its n x n pair-force scratch in the file-scope device
+// array below instead of a context buffer.  The caller passes device pointers
+// for the inputs and outputs; the function calls no cudaMalloc/cudaFree and no
+// allocating library routine.
+//
+// Limit: n <= D4_NOALLOC_MAX_N (1024), i.e. 8 MiB of scratch, held on every
+// GPU that loads the library until the process exits.  Every call shares the
+// array and it keeps the last call's contents; every entry a call reads is
+// written by the same call first, so nothing needs clearing, but calls that
+// overlap on the GPU (different streams, or different host threads) race on
+// it and must be serialised by the caller.  The first call on a device looks
+// up the array's device address (cudaGetSymbolAddress) with that device
+// current; make that first call before any stream capture begins.
+static __device__ __align__(256) double g_noalloc_pair_force[D4_NOALLOC_MAX_N * D4_NOALLOC_MAX_N];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress,
+                                 double *v, double *tol, double min_prec_sq, void *stream) {
+    if (n < 2 || n % 2 != 0 || !x || !y || !v) return D4_ERR_ARG;
+    if (n > D4_NOALLOC_MAX_N) return D4_ERR_ARG;  // scratch holds at most 1024 x 1024 forces
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return D4_ERR_CUDA;
+    double *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_pair_force) != cudaSuccess || !p)
+                return D4_ERR_CUDA;
+            g_noalloc_addr[dev] = static_cast<double *>(p);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    using namespace d4;
+    PairArgs a;
+    a.n = n;
+    a.x = x;
+    a.y = y;
+    a.F = scratch;
+    a.A = nullptr;
+    a.tol = tol;
+    a.min_prec_sq = min_prec_sq;
+    a.h = 0;
+    a.cut_sq = a.cutoff = a.range_sq = a.one_per_cut_sq = 0;
+    a.heaviside = 0;
+    k_pairs64<false><<<pair_blocks(n), dim3(kTile, 8), 0, st>>>(a);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) return D4_ERR_CUDA;
+    k_rows_speed64<<<blocks(n, 128), 128, 0, st>>>(n, scratch, ext_stress, v);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaGetLastError() != cudaSuccess) return D4_ERR_CUDA;
+    return D4_OK;
+}

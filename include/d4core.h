@@ -193,6 +193,26 @@ int d4_profile_read(void *ctx, double *ms, long long *calls);
 /* Number of kernels this library has launched in the process so far. */
 long long d4_kernel_launches(void);
 
+/* Allocation-free FP64 stress sweep (no counterpart in the reference: an
+ * addition of this library).  For callers that cannot allocate device memory,
+ * such as code running under CUDA-graph stream capture, real-time loops that
+ * must not wait on an allocator, or hosts whose device memory belongs to
+ * another framework's allocator.  Same result as d4_speeds: speeds v[n] and the
+ * tolerance update of tol[n] (may be null; starts from the caller's values,
+ * clamped below min_prec_sq as PrecisionHandler::updateTolerance does) for
+ * positions x[n], y[n] in internal order at external stress ext_stress.  All
+ * pointers are DEVICE pointers owned by the caller; the work is queued on
+ * `stream` (a cudaStream_t, null for the default stream) and the call returns
+ * without waiting.  The n x n scratch is a file-scope device array of
+ * D4_NOALLOC_MAX_N^2 doubles (8 MiB) that every GPU loading the library holds
+ * until exit: n > D4_NOALLOC_MAX_N is rejected with D4_ERR_ARG, as are odd n.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * must come before any stream capture; calls share the array, so calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+#define D4_NOALLOC_MAX_N 1024
+int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress, double *v,
+                      double *tol, double min_prec_sq, void *stream);
+
 /* Single field evaluations on the device (FP64 path), for checks. */
 int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
                   double *xy_diff_x);
