@@ -101,7 +101,8 @@ void free_all(Ctx *c) {
     void *bufs[] = {c->x0, c->y, c->xb, c->xh, c->x2, c->xs_tmp, c->ys_tmp, c->v_init,
                     c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
                     c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red,
-                    c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2};
+                    c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2,
+                    c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->h_red) cudaFreeHost(c->h_red);
@@ -327,13 +328,23 @@ int d4_create(void **out, int n, const d4_params *p) {
         D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
         D4_CUDA_OK(cudaMemset(c->dvec, 0, sizeof(double) * n));
         D4_CUDA_OK(cudaMemset(c->flags, 0, sizeof(int) * d4::kFlagCount));
-        d4::init_lu64();
+        c->lu_grid = d4::coop_grid_size(n);
+        if (c->lu_grid < 0) throw d4::StateError("n too large for the cooperative LU");
+        dalloc(&c->lu_p0, (size_t)n * 32);
+        dalloc(&c->lu_q, (size_t)n * 64);
+        c->lu_mask_words = nblk * 33 + 8;
+        dalloc(&c->lu_mask, (size_t)c->lu_mask_words);
+        dalloc(&c->lu_bar, 64);
         d4::reset_tol64(*c);
         sync(*c);
     } catch (const CudaError &e) {
         free_all(c);
         delete c;
         return D4_ERR_CUDA;
+    } catch (const d4::StateError &e) {
+        free_all(c);
+        delete c;
+        return D4_ERR_STATE;
     }
     *out = c;
     return D4_OK;

@@ -21,6 +21,7 @@ constexpr int kMaxSolveN = 8192;   // x and g of the one-CTA solve live in share
 enum FlagSlot {
     kFlagNeedPivot = 0,  // fast LU met |a_ik| > |a_kk| or a_kk == 0: partial pivoting would swap
     kFlagSingular = 1,   // pivoted LU met an exact zero pivot
+    kFlagBarrierTimeout = 2,  // a bounded grid-barrier wait gave up
     kFlagCount = 8
 };
 
@@ -83,6 +84,11 @@ struct Ctx {
     unsigned wave_epoch = 0;
     int *wave_err = nullptr;
     double *xw1 = nullptr, *xw2 = nullptr;
+    // cooperative LU: saved block columns, pre-division values, per-pass masks,
+    // grid barrier words
+    double *lu_p0 = nullptr, *lu_q = nullptr;
+    unsigned *lu_mask = nullptr, *lu_bar = nullptr;
+    int lu_mask_words = 0, lu_grid = 0;
 
     RunState rs;
     Prof prof;
@@ -120,8 +126,8 @@ void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double 
 // ---- FP64 factorisation and solves (d4_lu64.cu) ----
 // Factorises A into LU; returns via flags whether the pivoted path ran and
 // whether the matrix is singular.  Host-synchronising.
-int factor64(Ctx &c);
-void init_lu64();  // once per process and device, before the first solve
+int factor64(Ctx &c);                 // d4_lu_coop64.cu
+int coop_grid_size(int n);            // CTAs of the cooperative LU (-1: n too large)
 enum GMode { kGBig = 0, kGHalf = 1, kGNewton = 2 };
 // g built from (gmode, hval, dvec, s_end, s_init, x_new, x_old); solve; out = base - dx.
 void solve_update64(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
