@@ -39,7 +39,7 @@ class Params(C.Structure):
 
 class AttemptResult(C.Structure):
     _fields_ = [("ratio", C.c_double), ("max_id", C.c_int), ("accepted", C.c_int),
-                ("singular", C.c_int), ("pivoted", C.c_int)]
+                ("singular", C.c_int), ("pivoted", C.c_int), ("refine_residual", C.c_double)]
 
 
 class RunResult(C.Structure):

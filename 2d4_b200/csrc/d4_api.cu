@@ -102,7 +102,9 @@ void free_all(Ctx *c) {
                     c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
                     c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red,
                     c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2,
-                    c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar};
+                    c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
+                    c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
+                    c->m_w1, c->m_resid};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->h_red) cudaFreeHost(c->h_red);
@@ -148,27 +150,37 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     const double t_1__ = t0 + h;
     const double t_1p2 = t0 + h / 2;
     int singular = 0, pivoted = 0;
+    const bool mixed = c.p.precision == D4_PREC_MIXED;
     auto jac = [&](const double *x, double hh, double ta, double tb, double *va, double *vb) {
         ProfScope ps(c, D4_CAT_JACOBIAN);
-        d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
+        if (mixed)
+            d4::jacobian32(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
+        else
+            d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
     };
     auto fac = [&]() {
         int st;
         {
             ProfScope ps(c, D4_CAT_FACTOR);
-            st = d4::factor64(c);
+            st = mixed ? d4::factor32(c) : d4::factor64(c);
         }
         singular |= st == D4_WARN_SINGULAR;
         pivoted += c.factor_pivoted;
     };
     auto spd = [&](const double *x, double t, double *v) {
         ProfScope ps(c, D4_CAT_SPEEDS);
-        d4::speeds64(c, x, c.y, ext_stress(pr, t), v);
+        if (mixed)
+            d4::speeds32(c, x, c.y, ext_stress(pr, t), v);
+        else
+            d4::speeds64(c, x, c.y, ext_stress(pr, t), v);
     };
     auto slv = [&](int gmode, double hv, const double *se, const double *si, const double *xn,
                    const double *xo, const double *base, double *out) {
         ProfScope ps(c, D4_CAT_SOLVE);
-        d4::solve_update64(c, gmode, hv, se, si, xn, xo, base, out);
+        if (mixed)
+            d4::solve_update32(c, gmode, hv, se, si, xn, xo, base, out);
+        else
+            d4::solve_update64(c, gmode, hv, se, si, xn, xo, base, out);
     };
     // stage I: one large step
     jac(c.x0, h, t0, t_1__, c.v_init, c.speed);
@@ -181,7 +193,10 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
         const double factor = (t_1p2 - t0) / (t_1__ - t0);
         {
             ProfScope ps(c, D4_CAT_RESCALE);
-            d4::jacobian_from_prev64(c, factor);
+            if (mixed)
+                d4::jacobian_from_prev32(c, factor);
+            else
+                d4::jacobian_from_prev64(c, factor);
         }
         fac();
         const double dif = ext_stress(pr, t_1p2) - ext_stress(pr, t_1__);
@@ -200,11 +215,16 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     d4::error_ratio64(c, c.xb, c.x2);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost,
                                c.stream));
-    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags + 7, c.wave_err, sizeof(int), cudaMemcpyDeviceToHost,
-                               c.stream));
+    int werr[5];
+    D4_CUDA_OK(cudaMemcpyAsync(werr, c.wave_err, sizeof(werr), cudaMemcpyDeviceToHost, c.stream));
     sync(c);
     if (c.prof.on) d4::prof_collect(c);
-    if (c.h_flags[7]) throw d4::StateError("triangular solve wavefront timed out");
+    if (werr[0]) {
+        c.err_detail = "triangular solve wavefront timed out: block " + std::to_string(werr[1]) +
+                       " waiting for block " + std::to_string(werr[2]) + " saw flag " +
+                       std::to_string(werr[3]) + ", expected " + std::to_string(werr[4]);
+        throw d4::StateError(c.err_detail.c_str());
+    }
     const int idx = (int)c.h_red[1];
     if (idx >= 0) c.selected_id = idx;
     res->ratio = c.h_red[0] / c.dipole_prec_sq;
@@ -212,7 +232,45 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     res->accepted = res->ratio < 1;
     res->singular = singular;
     res->pivoted = pivoted;
+    res->refine_residual = 0;
+    if (mixed) {
+        unsigned long long rb[16];
+        D4_CUDA_OK(cudaMemcpy(rb, c.m_resid, sizeof(rb), cudaMemcpyDeviceToHost));
+        double worst = 0;
+        for (int k = 0; k < 8; ++k) {
+            double r, g;
+            std::memcpy(&r, &rb[2 * k], 8);
+            std::memcpy(&g, &rb[2 * k + 1], 8);
+            if (g > 0) worst = std::max(worst, r / g);
+        }
+        res->refine_residual = worst;
+        D4_CUDA_OK(cudaMemset(c.m_resid, 0, sizeof(rb)));
+    }
     return D4_OK;
+}
+
+// Stress sweep of the context's form (FP64 buffers exist only in the FP64 form).
+void sweep_speeds(Ctx &c, const double *x, const double *y, double ext, double *v) {
+    if (c.p.precision == D4_PREC_MIXED)
+        d4::speeds32(c, x, y, ext, v);
+    else
+        d4::speeds64(c, x, y, ext, v);
+}
+
+// Device matrix (FP64, or the mixed form's FP32 widened) to a host buffer.
+void copy_matrix_out(Ctx &c, double *dst) {
+    if (!dst) return;
+    const size_t nn = (size_t)c.n * c.n;
+    if (c.p.precision == D4_PREC_MIXED) {
+        std::vector<float> tmp(nn);
+        D4_CUDA_OK(cudaMemcpyAsync(tmp.data(), c.A32, sizeof(float) * nn, cudaMemcpyDeviceToHost,
+                                   c.stream));
+        sync(c);
+        for (size_t k = 0; k < nn; ++k) dst[k] = tmp[k];
+    } else {
+        D4_CUDA_OK(cudaMemcpyAsync(dst, c.A, sizeof(double) * nn, cudaMemcpyDeviceToHost,
+                                   c.stream));
+    }
 }
 
 double host_abs_sum(const std::vector<double> &v) {
@@ -272,7 +330,7 @@ int d4_create(void **out, int n, const d4_params *p) {
     if (n < 2 || n % 2 != 0 || n > d4::kMaxSolveN) return D4_ERR_ARG;
     if (p->weight_function != 'c' && p->weight_function != 'p' && p->weight_function != 'm')
         return D4_ERR_ARG;
-    if (p->precision != D4_PREC_FP64) return D4_ERR_ARG;
+    if (p->precision != D4_PREC_FP64 && p->precision != D4_PREC_MIXED) return D4_ERR_ARG;
     Ctx *c = new (std::nothrow) Ctx();
     if (!c) return D4_ERR_NOMEM;
     try {
@@ -306,9 +364,25 @@ int d4_create(void **out, int n, const d4_params *p) {
                            &c->v_init, &c->v_init2, &c->speed, &c->speed2, &c->dvec,
                            &c->dvec_new, &c->fac, &c->dx, &c->tol};
         for (double **v : vecs) dalloc(v, (size_t)n);
-        dalloc(&c->A, nn);
-        dalloc(&c->LU, nn);
-        dalloc(&c->F, nn);
+        const bool mixed = p->precision == D4_PREC_MIXED;
+        dalloc(&c->A, mixed ? 1 : nn);
+        dalloc(&c->LU, mixed ? 1 : nn);
+        dalloc(&c->F, mixed ? 1 : nn);
+        if (mixed) {
+            dalloc(&c->A32, nn);
+            dalloc(&c->LU32, nn);
+            dalloc(&c->lu32_p0, (size_t)n * 32);
+            dalloc(&c->lu32_q, (size_t)n * 64);
+            double **mv[] = {&c->m_vacc, &c->m_subacc, &c->m_g, &c->m_r, &c->m_dx};
+            for (double **v : mv) dalloc(v, (size_t)n);
+            dalloc(&c->m_c32, (size_t)n);
+            dalloc(&c->m_w1, (size_t)n);
+            dalloc(&c->m_resid, 16);
+            D4_CUDA_OK(cudaMemset(c->m_resid, 0, sizeof(unsigned long long) * 16));
+            D4_CUDA_OK(cudaMemset(c->A32, 0, sizeof(float) * nn));
+            c->lu32_grid = d4::coop_grid_size32(n);
+            if (c->lu32_grid < 0) throw d4::StateError("n too large for the cooperative LU");
+        }
         dalloc(&c->piv, (size_t)n);
         dalloc(&c->perm, (size_t)n);
         dalloc(&c->flags, (size_t)d4::kFlagCount);
@@ -316,16 +390,18 @@ int d4_create(void **out, int n, const d4_params *p) {
         const int nblk = (n + 31) / 32;
         dalloc(&c->wave_done, (size_t)nblk);
         dalloc(&c->wave_done2, (size_t)nblk);
-        dalloc(&c->wave_err, 1);
+        dalloc(&c->wave_err, 8);
         dalloc(&c->xw1, (size_t)n);
         dalloc(&c->xw2, (size_t)n);
         D4_CUDA_OK(cudaMemset(c->wave_done, 0, sizeof(unsigned) * nblk));
         D4_CUDA_OK(cudaMemset(c->wave_done2, 0, sizeof(unsigned) * nblk));
-        D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int)));
+        D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_red, sizeof(double) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_flags, sizeof(int) * d4::kFlagCount));
-        D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
-        D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
+        if (!mixed) {
+            D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
+            D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
+        }
         D4_CUDA_OK(cudaMemset(c->dvec, 0, sizeof(double) * n));
         D4_CUDA_OK(cudaMemset(c->flags, 0, sizeof(int) * d4::kFlagCount));
         c->lu_grid = d4::coop_grid_size(n);
@@ -411,7 +487,10 @@ int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, doub
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, x);
     upload(*c, c->ys_tmp, y);
-    d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
+    if (c->p.precision == D4_PREC_MIXED)
+        d4::speeds32(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
+    else
+        d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
     download(*c, v, c->speed2);
     if (tol) download(*c, tol, c->tol);
     sync(*c);
@@ -427,15 +506,17 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, x);
     upload(*c, c->ys_tmp, y);
-    d4::jacobian64(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
-                   ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
+    if (c->p.precision == D4_PREC_MIXED)
+        d4::jacobian32(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
+                       ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
+    else
+        d4::jacobian64(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
+                       ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
     download(*c, v_a, c->v_init);
     download(*c, v_b, c->speed);
     if (dvec) download(*c, dvec, c->dvec);
     if (tol) download(*c, tol, c->tol);
-    if (a_colmajor)
-        D4_CUDA_OK(cudaMemcpyAsync(a_colmajor, c->A, sizeof(double) * (size_t)c->n * c->n,
-                                   cudaMemcpyDeviceToHost, c->stream));
+    copy_matrix_out(*c, a_colmajor);
     sync(*c);
     return D4_OK;
     D4_GUARD_END(c)
@@ -445,11 +526,12 @@ int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *
     Ctx *c = (Ctx *)ctx;
     if (!c) return D4_ERR_ARG;
     D4_GUARD_BEGIN
-    d4::jacobian_from_prev64(*c, factor);
+    if (c->p.precision == D4_PREC_MIXED)
+        d4::jacobian_from_prev32(*c, factor);
+    else
+        d4::jacobian_from_prev64(*c, factor);
     if (dvec) download(*c, dvec, c->dvec);
-    if (a_colmajor)
-        D4_CUDA_OK(cudaMemcpyAsync(a_colmajor, c->A, sizeof(double) * (size_t)c->n * c->n,
-                                   cudaMemcpyDeviceToHost, c->stream));
+    copy_matrix_out(*c, a_colmajor);
     sync(*c);
     return D4_OK;
     D4_GUARD_END(c)
@@ -458,6 +540,7 @@ int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *
 int d4_set_matrix(void *ctx, const double *a_colmajor) {
     Ctx *c = (Ctx *)ctx;
     if (!c || !a_colmajor) return D4_ERR_ARG;
+    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_set_matrix: FP64 form only");
     D4_GUARD_BEGIN
     D4_CUDA_OK(cudaMemcpyAsync(c->A, a_colmajor, sizeof(double) * (size_t)c->n * c->n,
                                cudaMemcpyHostToDevice, c->stream));
@@ -470,6 +553,7 @@ int d4_factor(void *ctx) {
     Ctx *c = (Ctx *)ctx;
     if (!c) return D4_ERR_ARG;
     D4_GUARD_BEGIN
+    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_factor: FP64 form only");
     return d4::factor64(*c);
     D4_GUARD_END(c)
 }
@@ -477,6 +561,7 @@ int d4_factor(void *ctx) {
 int d4_solve(void *ctx, const double *g, double *dx) {
     Ctx *c = (Ctx *)ctx;
     if (!c || !g || !dx) return D4_ERR_ARG;
+    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_solve: FP64 form only");
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, g);
     d4::solve_plain64(*c, c->xs_tmp);
@@ -678,7 +763,7 @@ int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
     const d4::RunState before = c->rs;
     D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
     // src/simulation.cpp:46: initial speeds (also seeds the tolerances)
-    d4::speeds64(*c, c->x0, c->y, ext_stress(p.protocol, c->sim_time), c->v_init);
+    sweep_speeds(*c, c->x0, c->y, ext_stress(p.protocol, c->sim_time), c->v_init);
     if (log.is_open()) {
         std::vector<double> hv(n);
         download(*c, hv.data(), c->v_init);
@@ -710,7 +795,7 @@ int d4_advance(void *ctx, long long accepted_steps, d4_run_result *res) {
     if (!c->rs.started) {
         start_state(c);
         // the first attempt's tolerances include the initial sweep of run()
-        d4::speeds64(*c, c->x0, c->y, ext_stress(c->p.protocol, c->sim_time), c->v_init);
+        sweep_speeds(*c, c->x0, c->y, ext_stress(c->p.protocol, c->sim_time), c->v_init);
     }
     const d4::RunState before = c->rs;
     D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));

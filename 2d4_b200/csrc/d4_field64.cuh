@@ -68,7 +68,7 @@ __device__ __forceinline__ double f_l(double dx, double c, double ch) {
 }
 
 // Taylor branch of f_0 for dx^2 + dy^2 <= 1e-6, src/Fields/Field.cpp:183-187.
-__device__ __noinline__ double f0_taylor(double dx2pi, double dy2pi) {
+static __device__ __noinline__ double f0_taylor(double dx2pi, double dy2pi) {
     double x2 = dx2pi * dx2pi, y2 = dy2pi * dy2pi;
     double x4 = pow(dx2pi, 4.0), y4 = pow(dy2pi, 4.0);
     double x6 = pow(dx2pi, 6.0), y6 = pow(dy2pi, 6.0);
@@ -98,7 +98,7 @@ __device__ __forceinline__ double f_dx_l(double dx, double c, double ch, double 
 }
 
 // Taylor branch of f_dx_0, src/Fields/Field.cpp:224-249.
-__device__ __noinline__ double fdx0_taylor(double dx, double dy) {
+static __device__ __noinline__ double fdx0_taylor(double dx, double dy) {
     double dx2pi = dx * 2 * kPi;
     double dy2pi = dy * kPi * 2;
     double x2 = dx2pi * dx2pi, y2 = dy2pi * dy2pi;

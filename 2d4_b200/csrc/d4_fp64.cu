@@ -352,6 +352,13 @@ void jacobian_from_prev64(Ctx &c, double factor) {
                                c.stream));
 }
 
+void half_weights64(Ctx &c, double factor) {
+    k_half_weights64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.dvec, factor,
+                                                             c.p.weight_function, c.dvec_new,
+                                                             c.fac);
+    check_launch("k_half_weights64");
+}
+
 void shift_speed64(Ctx &c, double *v, double dif) {
     k_shift_speed64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, v, dif);
     check_launch("k_shift_speed64");

@@ -49,7 +49,7 @@ struct Ctx {
     d4_params p{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
+    std::string err, err_detail;
 
     // derived scalars (host, reference rounding)
     double min_prec_sq = 0, dipole_prec_sq = 1;
@@ -90,6 +90,16 @@ struct Ctx {
     unsigned *lu_mask = nullptr, *lu_bar = nullptr;
     int lu_mask_words = 0, lu_grid = 0;
 
+    // mixed form: FP32 matrix and factors, FP64 accumulators and refinement
+    float *A32 = nullptr, *LU32 = nullptr, *lu32_p0 = nullptr, *lu32_q = nullptr;
+    int lu32_grid = 0;
+    double *m_vacc = nullptr, *m_subacc = nullptr, *m_g = nullptr, *m_r = nullptr,
+           *m_dx = nullptr;
+    float *m_c32 = nullptr, *m_w1 = nullptr;
+    unsigned long long *m_resid = nullptr;  // 8 pairs (max |r|, max |g|) of recent solves
+    int m_resid_count = 0;
+    int ir_iters = 2;
+
     RunState rs;
     Prof prof;
 };
@@ -115,6 +125,7 @@ void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v);
 void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
                 double *v_a, double *v_b);
 void jacobian_from_prev64(Ctx &c, double factor);
+void half_weights64(Ctx &c, double factor);  // dvec_new and fac of the half step
 void shift_speed64(Ctx &c, double *v, double dif);
 void reset_tol64(Ctx &c);
 void error_ratio64(Ctx &c, const double *xb, const double *x2);  // -> red[0], red[1]
@@ -134,6 +145,16 @@ void solve_update64(Ctx &c, int gmode, double hval, const double *s_end, const d
                     const double *x_new, const double *x_old, const double *base, double *out);
 // Plain solve of A dx = g (g on device, dx written to c.dx).
 void solve_plain64(Ctx &c, const double *g);
+
+// ---- mixed form (d4_mixed.cu) ----
+void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v);
+void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
+                double *v_a, double *v_b);
+void jacobian_from_prev32(Ctx &c, double factor);
+int factor32(Ctx &c);
+int coop_grid_size32(int n);
+void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
+                    const double *x_new, const double *x_old, const double *base, double *out);
 
 }  // namespace d4
 

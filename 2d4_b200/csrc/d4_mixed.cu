@@ -1,0 +1,394 @@
+// d4_mixed.cu: the mixed-precision form of the implicit step.
+//
+// Pair stress and gradient in FP32 (d4_field32.cuh: compensated image sums,
+// cancellation-free central image), each unique pair once per sweep, summed
+// into FP64 accumulators.  The dense Jacobian A = I + D J is kept in FP32 and
+// factorised in FP32 (the cooperative LU of d4_lu_coop.cuh).  FP64 is kept for
+// positions, speeds, residuals g, d_i, the position updates and the error ratio;
+// each solve is refined in FP64 against the stored FP32 matrix:
+//     dx = 0, r = g;  repeat: c = LU32 \ r;  dx += c;  r = g - A32 dx
+// so the solution of A32 dx = g is accurate to FP64 rounding times cond(A).
+#include <cstdint>
+
+#include "d4_field32.cuh"
+#include "d4_field64.cuh"
+#include "d4_lu_coop.cuh"
+#include "d4_trsv.cuh"
+
+namespace d4 {
+namespace {
+
+__device__ __forceinline__ double bsign(int i, int n) { return i < n / 2 ? 1.0 : -1.0; }
+
+__device__ __forceinline__ void tol_min(double *tol, int idx, double d) {
+    atomicMin(reinterpret_cast<unsigned long long *>(tol + idx),
+              static_cast<unsigned long long>(__double_as_longlong(d)));
+}
+
+__device__ __forceinline__ void tile_of(int t, int T, int &ti, int &tj) {
+    int r = 0, rem = t;
+    while (rem >= T - r) {
+        rem -= T - r;
+        ++r;
+    }
+    ti = r;
+    tj = r + rem;
+}
+
+struct Pair32Args {
+    int n;
+    const double *x, *y;
+    double *vacc;    // FP64 sum of signed forces per dislocation (zeroed before)
+    double *subacc;  // FP64 sum of -J_ij per row (zeroed before; fused sweep)
+    float *A;        // raw J entries (fused sweep)
+    double *tol;
+    double min_prec_sq, h, cut_sq, cutoff, range_sq, one_per_cut_sq;
+    int heaviside;
+};
+
+// Unique pairs in 32x32 tiles (upper triangle); lanes walk i, threadIdx.y
+// steps j.  Row sums over the tile's j go through shared memory, column sums
+// over i through warp shuffles; one FP64 atomic per row and tile.
+template <bool kJac>
+__global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
+    const int T = (a.n + 31) / 32;
+    int ti, tj;
+    tile_of(blockIdx.x, T, ti, tj);
+    __shared__ double sxi[32], syi[32], sxj[32], syj[32];
+    __shared__ double rs[8][33], rj[8][33];
+    __shared__ float sv[kJac ? 32 : 1][kJac ? 33 : 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = ti * 32, j0 = tj * 32;
+    if (ty == 0) {
+        const int i = i0 + tx, j = j0 + tx;
+        sxi[tx] = i < a.n ? a.x[i] : 0;
+        syi[tx] = i < a.n ? a.y[i] : 0;
+        sxj[tx] = j < a.n ? a.x[j] : 0;
+        syj[tx] = j < a.n ? a.y[j] : 0;
+    }
+    __syncthreads();
+    const int i = i0 + tx;
+    const double bi = bsign(i, a.n);
+    double row_f = 0, row_j = 0, row_min = 1e300;
+    for (int lj = ty; lj < 32; lj += 8) {
+        const int j = j0 + lj;
+        double f = 0, fj = 0;
+        float v = 0.f;
+        const bool ok = i < a.n && j < a.n && i < j;
+        if (ok) {
+            const double dx = f64::normalize(sxi[tx] - sxj[lj]);
+            const double dy = f64::normalize(syi[tx] - syj[lj]);
+            const double dist_sq = dx * dx + dy * dy;
+            if (a.tol && dist_sq < a.min_prec_sq) {
+                row_min = fmin(row_min, dist_sq);
+                tol_min(a.tol, j, dist_sq);
+            }
+            float s, sd;
+            f32::field<kJac>((float)dx, (float)dy, s, sd);
+            const double bj = bsign(j, a.n);
+            f = (double)s * bi * bj;
+            if (kJac && dist_sq < a.range_sq * a.cut_sq) {
+                double vv = a.h * bj * bi * (double)sd;
+                if (!a.heaviside && dist_sq > a.cut_sq) {
+                    const double t = sqrt(dist_sq) - a.cutoff;
+                    vv *= exp(-(t * t) * a.one_per_cut_sq);
+                }
+                v = (float)vv;
+                fj = vv;
+            }
+            if (kJac) a.A[(size_t)i + (size_t)j * a.n] = v;
+        }
+        if (kJac) sv[tx][lj] = v;
+        row_f += f;
+        row_j += fj;
+        // column sums for row j: -f and -J, reduced over the warp's lanes (i)
+        double cf = -f, cj = fj;
+        for (int o = 16; o > 0; o >>= 1) {
+            cf += __shfl_down_sync(0xffffffffu, cf, o);
+            if (kJac) cj += __shfl_down_sync(0xffffffffu, cj, o);
+        }
+        if (tx == 0 && j < a.n) {
+            if (cf != 0) atomicAdd(a.vacc + j, cf);
+            if (kJac && cj != 0) atomicAdd(a.subacc + j, -cj);
+        }
+    }
+    if (a.tol && i < a.n && row_min < a.min_prec_sq) tol_min(a.tol, i, row_min);
+    rs[ty][tx] = row_f;
+    rj[ty][tx] = row_j;
+    __syncthreads();
+    if (ty == 0 && i < a.n) {
+        double sf = 0, sj = 0;
+        for (int k = 0; k < 8; ++k) {
+            sf += rs[k][tx];
+            sj += rj[k][tx];
+        }
+        if (sf != 0) atomicAdd(a.vacc + i, sf);
+        if (kJac && sj != 0) atomicAdd(a.subacc + i, -sj);
+    }
+    if (kJac) {
+        const int j = j0 + tx;
+        for (int li = ty; li < 32; li += 8) {
+            const int ii = i0 + li;
+            if (ii < a.n && j < a.n && ii < j) a.A[(size_t)j + (size_t)ii * a.n] = sv[li][tx];
+        }
+    }
+}
+
+__global__ void k_speed_fin32(int n, const double *vacc, double ext, double *v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = vacc[i] + ext * bsign(i, n);
+}
+
+// Row i: speeds at both times, d_i = weight(subSum_i), row scale and diagonal.
+__global__ void k_jac_fin32(int n, const double *vacc, const double *subacc, double ext_a,
+                            double ext_b, double *v_a, double *v_b, double *dvec, double *sc,
+                            float *A, char wfn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double b = bsign(i, n);
+    v_a[i] = vacc[i] + ext_a * b;
+    v_b[i] = vacc[i] + ext_b * b;
+    const double sub = subacc[i];
+    const double d = f64::weight(sub, wfn);
+    dvec[i] = d;
+    const double s = (1 + d) / 2;
+    sc[i] = s;
+    A[(size_t)i + (size_t)i * n] = (float)(sub * s + 1);
+}
+
+// A_rc *= sc_r off the diagonal (column-major, 2-D grid).
+__global__ void k_scale_rows32(int n, float *A, const double *sc) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r < n && r != c) A[(size_t)r + (size_t)c * n] = (float)((double)A[(size_t)r + (size_t)c * n] * sc[r]);
+}
+
+// Half-step rescale on the FP32 matrix (src/simulation.cpp:584-594).
+__global__ void k_half_rescale32(int n, float *A, const double *fac) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r >= n) return;
+    const double f = fac[r];
+    const double e = A[(size_t)r + (size_t)c * n];
+    A[(size_t)r + (size_t)c * n] = (float)((r == c) ? 1 + (e - 1) / 2 * f : e / 2 * f);
+}
+
+// g of the stage (as the FP64 form), r = g, dx = 0.
+__global__ void k_ir_init(int n, trsv::GArgs ga, double *g, double *r, double *dx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double gi = trsv::g_of(ga, i);
+    g[i] = gi;
+    r[i] = gi;
+    dx[i] = 0;
+}
+
+// dx += c (float correction), r = g (reset before the matrix product).
+__global__ void k_ir_accum(int n, const float *c, const double *g, double *dx, double *r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dx[i] += (double)c[i];
+    r[i] = g[i];
+}
+
+// r -= A32 dx over a chunk of columns per block (FP64 accumulation).
+__global__ void __launch_bounds__(256) k_gemv_sub32(int n, const float *__restrict__ A,
+                                                    const double *__restrict__ dx, double *r,
+                                                    int chunk) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c0 = blockIdx.y * chunk, c1 = min(n, c0 + chunk);
+    if (i >= n) return;
+    double s = 0;
+    for (int c = c0; c < c1; ++c) s += (double)__ldg(A + (size_t)i + (size_t)c * n) * dx[c];
+    atomicAdd(r + i, -s);
+}
+
+// max |r| and max |g| into out[0], out[1] (as ordered bits of non-negatives).
+__global__ void k_absmax2(int n, const double *r, const double *g, unsigned long long *out) {
+    double m1 = 0, m2 = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        m1 = fmax(m1, fabs(r[i]));
+        m2 = fmax(m2, fabs(g[i]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m1 = fmax(m1, __shfl_down_sync(0xffffffffu, m1, o));
+        m2 = fmax(m2, __shfl_down_sync(0xffffffffu, m2, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, (unsigned long long)__double_as_longlong(m1));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong(m2));
+    }
+}
+
+// dx -> out = base - dx, with the singular-matrix fix of src/simulation.cpp:646-658.
+__global__ void k_ir_apply(int n, const double *dx, const int *flags, const double *base,
+                           double *out, double *dx_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = dx[i];
+    if (flags[kFlagSingular] && !((-1 < d) && (d < 1))) d = 0;
+    if (dx_out) dx_out[i] = d;
+    out[i] = base[i] - d;
+}
+
+inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+static Pair32Args pair32(Ctx &c, const double *x, const double *y) {
+    Pair32Args a;
+    a.n = c.n;
+    a.x = x;
+    a.y = y;
+    a.vacc = c.m_vacc;
+    a.subacc = c.m_subacc;
+    a.A = c.A32;
+    a.tol = c.use_dipole ? c.tol : nullptr;
+    a.min_prec_sq = c.min_prec_sq;
+    a.h = 0;
+    a.cut_sq = c.cutoff_sq;
+    a.cutoff = c.cutoff;
+    a.range_sq = c.range_sq;
+    a.one_per_cut_sq = 1 / c.cutoff_sq;
+    a.heaviside = c.p.heaviside_cutoff;
+    return a;
+}
+
+static int pair_tiles(int n) {
+    const int T = (n + 31) / 32;
+    return T * (T + 1) / 2;
+}
+
+void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v) {
+    D4_CUDA_OK(cudaMemsetAsync(c.m_vacc, 0, sizeof(double) * c.n, c.stream));
+    Pair32Args a = pair32(c, x, y);
+    k_pairs32<false><<<pair_tiles(c.n), dim3(32, 8), 0, c.stream>>>(a);
+    check_launch("k_pairs32<speeds>");
+    k_speed_fin32<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_vacc, ext, v);
+    check_launch("k_speed_fin32");
+}
+
+void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
+                double *v_a, double *v_b) {
+    D4_CUDA_OK(cudaMemsetAsync(c.m_vacc, 0, sizeof(double) * c.n, c.stream));
+    D4_CUDA_OK(cudaMemsetAsync(c.m_subacc, 0, sizeof(double) * c.n, c.stream));
+    Pair32Args a = pair32(c, x, y);
+    a.h = h;
+    k_pairs32<true><<<pair_tiles(c.n), dim3(32, 8), 0, c.stream>>>(a);
+    check_launch("k_pairs32<jacobian>");
+    k_jac_fin32<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_vacc, c.m_subacc, ext_a, ext_b,
+                                                     v_a, v_b, c.dvec, c.fac, c.A32,
+                                                     c.p.weight_function);
+    check_launch("k_jac_fin32");
+    k_scale_rows32<<<dim3(nb(c.n, 256), c.n), 256, 0, c.stream>>>(c.n, c.A32, c.fac);
+    check_launch("k_scale_rows32");
+}
+
+void jacobian_from_prev32(Ctx &c, double factor) {
+    half_weights64(c, factor);  // dvec_new, fac
+    k_half_rescale32<<<dim3(nb(c.n, 256), c.n), 256, 0, c.stream>>>(c.n, c.A32, c.fac);
+    check_launch("k_half_rescale32");
+    D4_CUDA_OK(cudaMemcpyAsync(c.dvec, c.dvec_new, sizeof(double) * c.n, cudaMemcpyDeviceToDevice,
+                               c.stream));
+}
+
+int factor32(Ctx &c) {
+    const int n = c.n;
+    D4_CUDA_OK(cudaMemsetAsync(c.flags, 0, sizeof(int) * kFlagCount, c.stream));
+    D4_CUDA_OK(cudaMemsetAsync(c.lu_bar, 0, sizeof(unsigned) * 64, c.stream));
+    D4_CUDA_OK(cudaMemsetAsync(c.lu_mask, 0, sizeof(unsigned) * c.lu_mask_words, c.stream));
+    D4_CUDA_OK(cudaMemcpyAsync(c.LU32, c.A32, sizeof(float) * (size_t)n * n,
+                               cudaMemcpyDeviceToDevice, c.stream));
+    coop::CoopArgs<float> a;
+    a.n = n;
+    a.A = c.LU32;
+    a.P0 = c.lu32_p0;
+    a.Q = c.lu32_q;
+    a.mask = c.lu_mask;
+    a.piv = c.piv;
+    a.flags = c.flags;
+    a.bar = c.lu_bar;
+    a.perm = c.perm;
+    void *args[] = {(void *)&a};
+    const void *kern = (const void *)coop::k_lu_coop<float>;
+    D4_CUDA_OK(cudaLaunchCooperativeKernel(kern, dim3(c.lu32_grid), dim3(coop::kThreads), args,
+                                           coop::kRowBufBytes<float>(), c.stream));
+    check_launch("k_lu_coop<float>");
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
+                               cudaMemcpyDeviceToHost, c.stream));
+    D4_CUDA_OK(cudaStreamSynchronize(c.stream));
+    if (c.h_flags[kFlagBarrierTimeout]) throw StateError("LU grid barrier timed out");
+    c.factor_singular = c.h_flags[kFlagSingular] != 0;
+    c.factor_pivoted = 0;
+    return c.factor_singular ? D4_WARN_SINGULAR : D4_OK;
+}
+
+int coop_grid_size32(int n) {
+    int dev = 0, sms = 0, per_sm = 0;
+    D4_CUDA_OK(cudaGetDevice(&dev));
+    D4_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    D4_CUDA_OK(cudaFuncSetAttribute(coop::k_lu_coop<float>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)coop::kRowBufBytes<float>()));
+    D4_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, coop::k_lu_coop<float>, coop::kThreads, coop::kRowBufBytes<float>()));
+    const int g = sms * (per_sm < 1 ? 1 : per_sm);
+    return g < (n + coop::kThreads - 1) / coop::kThreads ? -1 : g;
+}
+
+// FP32 wavefront solve of LU32 c = r (r FP64 in, c FP32 out).
+static void solve32_once(Ctx &c, const double *r, float *out) {
+    const int nblk = (c.n + 31) / 32;
+    unsigned e1 = ++c.wave_epoch;
+    unsigned e2 = ++c.wave_epoch;
+    trsv::GArgs g{};
+    g.gmode = -1;
+    g.g_in = r;
+    const float *xin_null = nullptr;
+    float *xw1 = c.m_w1, *xw2 = out;
+    void *args1[] = {(void *)&c.n, (void *)&c.LU32, (void *)&c.perm, (void *)&c.flags, (void *)&g,
+                     (void *)&xw1, (void *)&xin_null, (void *)&c.wave_done, (void *)&e1,
+                     (void *)&c.wave_err};
+    const void *fwd = (const void *)trsv::k_trsv_wave<true, float>;
+    const void *bwd = (const void *)trsv::k_trsv_wave<false, float>;
+    D4_CUDA_OK(cudaLaunchCooperativeKernel(fwd, dim3(nblk), dim3(trsv::kWaveThreads), args1, 0,
+                                           c.stream));
+    check_launch("k_trsv_wave<fwd, float>");
+    void *args2[] = {(void *)&c.n, (void *)&c.LU32, (void *)&c.perm, (void *)&c.flags, (void *)&g,
+                     (void *)&xw2, (void *)&xw1, (void *)&c.wave_done2, (void *)&e2,
+                     (void *)&c.wave_err};
+    D4_CUDA_OK(cudaLaunchCooperativeKernel(bwd, dim3(nblk), dim3(trsv::kWaveThreads), args2, 0,
+                                           c.stream));
+    check_launch("k_trsv_wave<bwd, float>");
+}
+
+void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
+                    const double *x_new, const double *x_old, const double *base, double *out) {
+    const int n = c.n;
+    trsv::GArgs ga{};
+    ga.gmode = gmode;
+    ga.hval = hval;
+    ga.dvec = c.dvec;
+    ga.s_end = s_end;
+    ga.s_init = s_init;
+    ga.x_new = x_new;
+    ga.x_old = x_old;
+    k_ir_init<<<nb(n, 256), 256, 0, c.stream>>>(n, ga, c.m_g, c.m_r, c.m_dx);
+    check_launch("k_ir_init");
+    const int chunk = 256;
+    for (int it = 0; it < c.ir_iters; ++it) {
+        solve32_once(c, c.m_r, c.m_c32);
+        k_ir_accum<<<nb(n, 256), 256, 0, c.stream>>>(n, c.m_c32, c.m_g, c.m_dx, c.m_r);
+        check_launch("k_ir_accum");
+        k_gemv_sub32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, c.stream>>>(n, c.A32, c.m_dx, c.m_r,
+                                                                         chunk);
+        check_launch("k_gemv_sub32");
+    }
+    k_absmax2<<<64, 256, 0, c.stream>>>(n, c.m_r, c.m_g, c.m_resid + 2 * c.m_resid_count);
+    check_launch("k_absmax2");
+    c.m_resid_count = (c.m_resid_count + 1) % 8;
+    k_ir_apply<<<nb(n, 256), 256, 0, c.stream>>>(n, c.m_dx, c.flags, base, out, c.dx);
+    check_launch("k_ir_apply");
+}
+
+}  // namespace d4

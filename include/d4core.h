@@ -88,7 +88,8 @@ typedef struct d4_params {
     double sub_config_times;      /* -T; 0: none */
     char sub_config_times_type;   /* -b: 'a' (default) or 'b' */
     d4_protocol protocol;
-    int precision;                /* D4_PREC_FP64 or D4_PREC_MIXED */
+    int precision;                /* D4_PREC_FP64 or D4_PREC_MIXED (d4_set_matrix,
+                                     d4_factor, d4_solve: FP64 form only) */
     int device;                   /* CUDA device ordinal */
 } d4_params;
 
@@ -99,6 +100,8 @@ typedef struct d4_attempt_result {
     int accepted;       /* ratio < 1 */
     int singular;       /* a factorisation met an exact zero pivot */
     int pivoted;        /* number of factorisations that needed row swaps */
+    double refine_residual; /* mixed form: worst max|g - A dx| / max|g| of the
+                               attempt's refined solves (0 for the FP64 form) */
 } d4_attempt_result;
 
 typedef struct d4_run_result {

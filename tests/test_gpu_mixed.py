@@ -1,0 +1,99 @@
+"""GPU checks of the mixed-precision form against the FP64 oracle (marked gpu).
+
+FP32 pair stress/gradient with compensated image sums, FP32 Jacobian and LU,
+FP64 residuals, refinement, positions and acceptance.  Tolerances: per-pair
+FP32 rounding (~1e-7 relative) for the sweeps and the matrix; the refined solve
+to 1e-10 relative residual; one attempt's positions to 1e-8; a fixed step
+sequence of 200 accepted steps to 1e-7 against the plain FP64 form.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def engine(pkg, x, y, **kw):
+    sd = pkg.SimulationData()
+    sd.set_positions(x, y)
+    sd.precision_mode = pkg._lib.D4_PREC_MIXED
+    for k, v in kw.items():
+        setattr(sd, k, v)
+    return pkg.Engine(sd)
+
+
+@pytest.mark.parametrize("n,seed", [(64, 1000), (256, 7), (1024, 1001)])
+def test_mixed_speeds(pkg, restated, n, seed):
+    x, y, _ = pkg.dconf.generate_internal(n, seed)
+    e = engine(pkg, x, y)
+    v, tol = e.speeds(x, y, 0.0)
+    p = restated.params()
+    mps, _, _, _ = restated.derived(p, n)
+    tol_o = np.full(n, mps)
+    vo = restated.speeds(x, y, 0.0, tol_o, mps)
+    assert np.abs(v - vo).max() / np.abs(vo).max() < 1e-6
+    assert np.array_equal(tol, tol_o)  # distances stay FP64
+
+
+def test_mixed_close_pairs(pkg, golden):
+    """Near-field pairs (r^2 <= 1e-6 uses the reference's Taylor branch): the
+    half-angle FP32 form keeps ~1e-6 relative accuracy there."""
+    x = np.array([0.1, 0.1 + 3e-4, -0.2, 0.3])
+    y = np.array([0.05, 0.05 - 2e-4, 0.2, -0.1])
+    import pyoracle
+    ro = pyoracle.Restated()
+    vo = ro.speeds(x, y, 0.0)
+    e = engine(pkg, x, y)
+    v, _ = e.speeds(x, y, 0.0)
+    assert np.abs(v - vo).max() / np.abs(vo).max() < 2e-6
+
+
+def test_mixed_jacobian(pkg, restated):
+    n = 256
+    x, y, _ = pkg.dconf.generate_internal(n, 7)
+    e = engine(pkg, x, y)
+    va, vb, a, d, _ = e.jacobian(x, y, 1e-4, 0.0, 1e-4)
+    p = restated.params()
+    mps, _, cut, cs = restated.derived(p, n)
+    vao, vbo, ao, do = restated.jacobian(x, y, 1e-4, 0.0, 0.0, cs, cut)
+    assert np.abs(a - ao).max() / np.abs(ao).max() < 2e-6
+    assert np.abs(d - do).max() < 1e-6
+
+
+@pytest.mark.parametrize("n,h", [(256, 5e-7), (1024, 2e-7)])
+def test_mixed_attempt(pkg, restated, n, h):
+    x, y, _ = pkg.dconf.generate_internal(n, 1002)
+    e = engine(pkg, x, y, external_stress=pkg.FixedRateProtocol(0.1, 0.0))
+    r, xb, xh, x2 = e.attempt(0.0, h)
+    p = restated.params(protocol=dict(kind=1, tau0=0.1, rate=0.0))
+    mps, _, _, _ = restated.derived(p, n)
+    xbo, xho, x2o, _, ro, io = restated.attempt(x, y, 0.0, h, p, np.full(n, mps))
+    assert np.abs(x2 - x2o).max() < 1e-8
+    assert np.abs(xb - xbo).max() < 1e-8
+    assert r.refine_residual < 1e-10
+    assert ro < 1  # a step size the error control accepts
+    assert abs(r.ratio - ro) <= 1e-3 * ro + 1e-12
+
+
+def test_mixed_fixed_steps_vs_fp64(pkg):
+    """200 accepted steps with the step size capped at h (P large, so the
+    dipole criterion decides the few rejections): mixed vs the plain FP64 form
+    along the same step sequence."""
+    n, h, steps = 256, 2e-6, 200
+    x, y, _ = pkg.dconf.generate_internal(n, 1002)
+    out = []
+    for mode in (pkg._lib.D4_PREC_FP64, pkg._lib.D4_PREC_MIXED):
+        sd = pkg.SimulationData()
+        sd.set_positions(x, y)
+        sd.precision_mode = mode
+        sd.precision = 1.0  # step size capped at h; the dipole criterion still rejects
+        sd.max_step_size_limited, sd.max_stepsize_limit, sd.step_size = True, h, h
+        sd.external_stress = pkg.FixedRateProtocol(0.1, 0.0)
+        e = pkg.Engine(sd)
+        r = e.advance(steps)
+        out.append((e.positions()[0], r))
+        e.close()
+    # the same sequence of attempted and accepted steps in both forms
+    assert out[0][1].attempts == out[1][1].attempts
+    assert out[0][1].failed_steps == out[1][1].failed_steps
+    d, _, _, _ = pkg.dconf.conf_compare(out[1][0], y, out[0][0], y)
+    assert d < 1e-7
