@@ -2,6 +2,7 @@
 // (double: plain form, --fmad=false; float: mixed form).  See d4_lu_coop64.cu.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "d4_internal.h"
 
@@ -12,8 +13,19 @@ constexpr int NB = 32;
 constexpr int kThreads = 256;
 constexpr long long kSpinLimit = 1ll << 24;  // x >= 64 ns each: > 1 s
 constexpr int kGenWord = 32;
+// Dynamic shared memory: the rows-below buffer, and for the FP32 form the four
+// tensor-core operand tiles (L21 and U12 as TF32 hi and lo parts, 16 KiB each,
+// 1 KiB aligned) plus the MMA completion barrier and the TMEM address slot.
+constexpr size_t kOpTileBytes = 128 * NB * 4;
 template <typename T>
-constexpr size_t kRowBufBytes() { return sizeof(T) * kThreads * (NB + 1); }
+__host__ __device__ constexpr size_t kRowBufRaw() { return sizeof(T) * kThreads * (NB + 1); }
+template <typename T>
+__host__ __device__ constexpr size_t kTcOffset() { return (kRowBufRaw<T>() + 1023) / 1024 * 1024; }
+template <typename T>
+__host__ __device__ constexpr size_t kRowBufBytes() {
+    return std::is_same<T, float>::value ? kTcOffset<T>() + 4 * kOpTileBytes + 1024 + 64
+                                         : kRowBufRaw<T>();
+}
 
 template <typename T>
 struct CoopArgs {
@@ -233,6 +245,99 @@ __device__ __noinline__ unsigned rows_below(const CoopArgs<T> &a, T *Q,
     return msk;
 }
 
+
+// ---------------------------------------------------------------------------
+// Tensor-core trailing update of the FP32 form (tcgen05, kind::tf32).
+//
+// Operand tiles live in shared memory in the canonical K-major layout without
+// swizzle: 8-row x 16-byte core matrices, the 8-row groups of a 4-wide K chunk
+// contiguous (stride 128 B), consecutive K chunks 16 groups apart (2048 B).
+// One instruction covers K = 8 (two chunks).  Each FP32 operand is split into
+// TF32 hi and lo parts and the product formed as hi*hi + hi*lo + lo*hi, which
+// keeps it close to FP32 accuracy (the update is memory-bound, so the three
+// MMAs cost nothing).  D (128 x 128 FP32) accumulates in 128 TMEM columns.
+namespace tc {
+
+constexpr uint32_t kLBO = 2048;  // K-chunk stride
+constexpr uint32_t kSBO = 128;   // 8-row group stride
+// kind::tf32, D F32, A and B TF32 K-major, N = 128, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+constexpr long long kWaitLimit = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(kLBO >> 4) << 16) |
+           ((uint64_t)(kSBO >> 4) << 32) | (1ull << 46);
+}
+
+// byte offset of element (row, k) of a 128 x 32 operand tile
+__device__ __forceinline__ uint32_t off(int row, int k) {
+    return (uint32_t)((((k >> 2) * 16 + (row >> 3)) * 128) + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+}
+
+__device__ __forceinline__ void commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(mbar) : "memory");
+}
+
+// Bounded wait for the barrier's phase `parity`; false if it gave up.
+__device__ __forceinline__ bool wait(uint32_t mbar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+        "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int t = 0; t < 32; ++t) v[t] = __uint_as_float(r[t]);
+}
+
+__device__ __forceinline__ void fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+}  // namespace tc
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     extern __shared__ __align__(16) unsigned char rowbuf_raw[];
@@ -255,6 +360,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     if (tid == 0) dead_s = 0;
     const int nblk = (n + NB - 1) / NB;
     for (int i = cta * kThreads + tid; i < n; i += G * kThreads) a.perm[i] = i;
+    constexpr bool kTc = std::is_same<T, float>::value;
+    unsigned char *tc_base = rowbuf_raw + kTcOffset<T>();
+    uint64_t *tc_mbar = reinterpret_cast<uint64_t *>(tc_base + 4 * kOpTileBytes);
+    uint32_t *tc_slot = reinterpret_cast<uint32_t *>(tc_base + 4 * kOpTileBytes + 64);
+    uint32_t tmem = 0, tc_phase = 0;
+    if (kTc) {
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;"
+                         ::"r"(tc::smem_u32(tc_slot)) : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(tc_mbar))
+                         : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        tmem = *tc_slot;
+    }
 
     // prologue: P0 = first block's columns
     for (size_t t = (size_t)cta * kThreads + tid; t < (size_t)n * NB; t += (size_t)G * kThreads) {
@@ -388,7 +514,97 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
         // ---------------------------------------------------------- update
         const int base = k0 + kw;
         const int rest = n - base;
-        if (rest > 0) {
+        if (kTc && rest > 0) {
+            const int nk0 = base, nkw = min(NB, n - base);  // next block's columns
+            const int tb = (rest + 127) / 128;
+            float *Ahi = reinterpret_cast<float *>(tc_base);
+            float *Alo = reinterpret_cast<float *>(tc_base + kOpTileBytes);
+            float *Bhi = reinterpret_cast<float *>(tc_base + 2 * kOpTileBytes);
+            float *Blo = reinterpret_cast<float *>(tc_base + 3 * kOpTileBytes);
+            for (int tile = cta; tile < tb * tb; tile += G) {
+                const int i0 = base + (tile % tb) * 128, j0 = base + (tile / tb) * 128;
+                // stage L21 (rows i0.., columns k0..) and U12 (rows k0.., columns j0..):
+                // all global loads first (independent), then split and store
+                {
+                    constexpr int kPer = 128 * NB / kThreads;  // 16 entries per thread
+                    float xa[kPer], xb[kPer];
+#pragma unroll
+                    for (int r = 0; r < kPer; ++r) {
+                        const int t = tid + r * kThreads;
+                        const int m = t & 127, k = t >> 7;
+                        const int gi = i0 + m;
+                        xa[r] = (k < kw && gi < n) ? (float)a.A[(size_t)gi + (size_t)(k0 + k) * n]
+                                                   : 0.f;
+                        const int k2 = t & 31, nn = t >> 5;
+                        const int gj = j0 + nn;
+                        xb[r] = (k2 < kw && gj < n) ? (float)a.A[(size_t)(k0 + k2) + (size_t)gj * n]
+                                                    : 0.f;
+                    }
+#pragma unroll
+                    for (int r = 0; r < kPer; ++r) {
+                        const int t = tid + r * kThreads;
+                        const uint32_t o = tc::off(t & 127, t >> 7) >> 2;
+                        const float hi = tc::to_tf32(xa[r]);
+                        Ahi[o] = hi;
+                        Alo[o] = tc::to_tf32(xa[r] - hi);
+                        const uint32_t o2 = tc::off(t >> 5, t & 31) >> 2;
+                        const float yh = tc::to_tf32(xb[r]);
+                        Bhi[o2] = yh;
+                        Blo[o2] = tc::to_tf32(xb[r] - yh);
+                    }
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (tid == 0) {
+                    tc::fence_after();
+                    const uint32_t ah = tc::smem_u32(Ahi), al = tc::smem_u32(Alo);
+                    const uint32_t bh = tc::smem_u32(Bhi), bl = tc::smem_u32(Blo);
+#pragma unroll
+                    for (int q = 0; q < NB / 8; ++q) {
+                        const uint32_t ko = q * 2 * tc::kLBO;
+                        tc::mma(tmem, tc::desc(ah + ko), tc::desc(bh + ko), q > 0 ? 1u : 0u);
+                        tc::mma(tmem, tc::desc(ah + ko), tc::desc(bl + ko), 1u);
+                        tc::mma(tmem, tc::desc(al + ko), tc::desc(bh + ko), 1u);
+                    }
+                    tc::commit(tc::smem_u32(tc_mbar));
+                }
+                const bool ok = tc::wait(tc::smem_u32(tc_mbar), tc_phase);
+                tc_phase ^= 1u;
+                if (!ok && tid == 0) atomicOr(&a.flags[kFlagBarrierTimeout], 1);
+                tc::fence_after();
+                {
+                    const int q4 = warp & 3, hf = warp >> 2;
+                    const int gi = i0 + 32 * q4 + lane;
+#pragma unroll 1
+                    for (int c = 0; c < 2; ++c) {
+                        const int cb = 64 * hf + 32 * c;
+                        float v[32];
+                        tc::ld32(tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)cb, v);
+                        if (gi < n) {
+                            // loads first (independent), then the stores
+                            T cv[32];
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const int gj = j0 + cb + t;
+                                cv[t] = gj < n ? a.A[(size_t)gi + (size_t)gj * n] : T(0);
+                            }
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const int gj = j0 + cb + t;
+                                if (gj < n) {
+                                    const T r = cv[t] - (T)v[t];
+                                    a.A[(size_t)gi + (size_t)gj * n] = r;
+                                    if (gj >= nk0 && gj < nk0 + nkw)
+                                        a.P0[(size_t)gi + (size_t)(gj - nk0) * n] = r;
+                                }
+                            }
+                        }
+                    }
+                }
+                tc::fence_before();
+                __syncthreads();
+            }
+        } else if (rest > 0) {
             const int tb = (rest + 63) / 64;
             const int nk0 = base, nkw = min(NB, n - base);  // next block's columns
             for (int tile = cta; tile < tb * tb; tile += G) {
@@ -440,6 +656,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             // never read from P0 (positions >= nk0 only)
         }
         grid_barrier(a.bar, a.flags, gen, &dead_s);
+    }
+    if (kTc) {
+        tc::fence_before();
+        __syncthreads();
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem)
+                         : "memory");
     }
 }
 
