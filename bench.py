@@ -223,6 +223,40 @@ def roofline(prof, n, hbm_gbs, fp64_tf):
                 peak_source="cuBLAS DGEMM 4096^3 measured in this run (FP64 peak)")
 
 
+def mixed_vs_fp64(pkg, steps=8, warmup=2, n=4096, seed=1002, tau=0.1):
+    """The metric's comparison: N=4096 (seed 1002, tau_ext = 0.1, default
+    precision), the plain FP64 form and the mixed form from the same start,
+    each timed over `steps` accepted steps (CUDA events, device time), and the
+    max position difference between the two after those steps (meaningful when
+    both took the same step sequence, reported as same_steps)."""
+    x, y, _ = pkg.dconf.generate_internal(n, seed)
+    out = {}
+    for name, mode in (("fp64", pkg._lib.D4_PREC_FP64), ("mixed", pkg._lib.D4_PREC_MIXED)):
+        sd = pkg.SimulationData()
+        sd.set_positions(x, y)
+        sd.precision_mode = mode
+        sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
+        eng = pkg.Engine(sd)
+        eng.advance(warmup)
+        eng.profile(True)
+        r = eng.advance(steps)
+        prof = eng.profile_read()
+        out[name] = dict(value=n * steps / r.device_seconds, attempts=int(r.attempts),
+                         failed=int(r.failed_steps), x=eng.positions()[0],
+                         ms_per_call={k: round(v[0] / max(v[1], 1), 3) for k, v in prof.items()})
+        eng.close()
+    d, _, _, _ = pkg.dconf.conf_compare(out["mixed"]["x"], y, out["fp64"]["x"], y)
+    return {"n": n, "tau_ext": tau, "steps": steps, "warmup": warmup,
+            "fp64_dislocation_steps_per_s": out["fp64"]["value"],
+            "mixed_dislocation_steps_per_s": out["mixed"]["value"],
+            "speedup": out["mixed"]["value"] / out["fp64"]["value"],
+            "same_steps": out["fp64"]["attempts"] == out["mixed"]["attempts"],
+            "attempts": [out["fp64"]["attempts"], out["mixed"]["attempts"]],
+            "max_position_diff_vs_fp64": d,
+            "fp64_ms_per_call": out["fp64"]["ms_per_call"],
+            "mixed_ms_per_call": out["mixed"]["ms_per_call"]}
+
+
 def run_reference_arm(args, wl):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -260,6 +294,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the N=4096 mixed vs FP64 leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -358,6 +393,11 @@ def main():
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "kernel_ms": {k: v[0] for k, v in prof.items()},
             "kernel_calls": {k: v[1] for k, v in prof.items()}}
+    if ws == 1 and not args.no_mixed:
+        try:
+            line["mixed_vs_fp64"] = mixed_vs_fp64(pkg)
+        except Exception as e:  # pragma: no cover
+            line["mixed_vs_fp64"] = {"unavailable": str(e)}
     if ws == 1 and not args.no_cpu_baseline:
         try:
             per_step = {64: 0.002, 1024: 0.5, 4096: 25.0}.get(n, 1.0)
