@@ -107,6 +107,7 @@ void free_all(Ctx *c) {
                     c->m_w1, c->m_resid};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    d4::sparse_free(*c);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_flags) cudaFreeHost(c->h_flags);
     for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
@@ -158,14 +159,18 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
         else
             d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
     };
-    auto fac = [&]() {
-        int st;
-        {
-            ProfScope ps(c, D4_CAT_FACTOR);
-            st = mixed ? d4::factor32(c) : d4::factor64(c);
-        }
+    const bool gmres = c.use_gmres != 0;
+    auto dense_fac = [&]() {
+        const int st = mixed ? d4::factor32(c) : d4::factor64(c);
         singular |= st == D4_WARN_SINGULAR;
         pivoted += c.factor_pivoted;
+    };
+    auto fac = [&]() {
+        ProfScope ps(c, D4_CAT_FACTOR);
+        if (gmres)
+            d4::sparse_prepare(c);
+        else
+            dense_fac();
     };
     auto spd = [&](const double *x, double t, double *v) {
         ProfScope ps(c, D4_CAT_SPEEDS);
@@ -177,6 +182,13 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     auto slv = [&](int gmode, double hv, const double *se, const double *si, const double *xn,
                    const double *xo, const double *base, double *out) {
         ProfScope ps(c, D4_CAT_SOLVE);
+        if (gmres) {
+            if (d4::sparse_solve_update(c, gmode, hv, se, si, xn, xo, base, out)) return;
+            if (!c.sp_dense_ready) {  // GMRES did not converge: dense LU of the same matrix
+                dense_fac();
+                c.sp_dense_ready = 1;
+            }
+        }
         if (mixed)
             d4::solve_update32(c, gmode, hv, se, si, xn, xo, base, out);
         else
@@ -322,6 +334,7 @@ void d4_default_params(d4_params *p) {
     p->sub_config_times_type = 'a';
     p->precision = D4_PREC_FP64;
     p->device = 0;
+    p->solver = D4_SOLVER_DENSE;
 }
 
 int d4_create(void **out, int n, const d4_params *p) {
@@ -331,6 +344,7 @@ int d4_create(void **out, int n, const d4_params *p) {
     if (p->weight_function != 'c' && p->weight_function != 'p' && p->weight_function != 'm')
         return D4_ERR_ARG;
     if (p->precision != D4_PREC_FP64 && p->precision != D4_PREC_MIXED) return D4_ERR_ARG;
+    if (p->solver < D4_SOLVER_DENSE || p->solver > D4_SOLVER_AUTO) return D4_ERR_ARG;
     Ctx *c = new (std::nothrow) Ctx();
     if (!c) return D4_ERR_NOMEM;
     try {
@@ -411,6 +425,8 @@ int d4_create(void **out, int n, const d4_params *p) {
         c->lu_mask_words = nblk * 33 + 8;
         dalloc(&c->lu_mask, (size_t)c->lu_mask_words);
         dalloc(&c->lu_bar, 64);
+        c->use_gmres = d4::gmres_selected(*c) ? 1 : 0;
+        if (c->use_gmres) d4::sparse_alloc(*c);
         d4::reset_tol64(*c);
         sync(*c);
     } catch (const CudaError &e) {
@@ -833,6 +849,17 @@ int d4_profile_read(void *ctx, double *ms, long long *calls) {
     }
     return D4_OK;
     D4_GUARD_END(c)
+}
+
+int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long long *fallbacks,
+                    long long *nnz) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !solves || !iterations || !fallbacks || !nnz) return D4_ERR_ARG;
+    *solves = c->sp_solves;
+    *iterations = c->sp_iters;
+    *fallbacks = c->sp_fallbacks;
+    *nnz = c->sp_nnz;
+    return D4_OK;
 }
 
 long long d4_kernel_launches(void) { return d4::g_launches.load(); }

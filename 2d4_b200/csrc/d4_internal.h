@@ -100,6 +100,16 @@ struct Ctx {
     int m_resid_count = 0;
     int ir_iters = 2;
 
+    // cutoff sparse path: CSR of the matrix and the GMRES work space
+    int use_gmres = 0;
+    int sp_grid = 0, sp_nch = 0, sp_cap = 0, sp_nnz = 0, sp_dense_ready = 0;
+    int *sp_cnt = nullptr, *sp_off = nullptr, *sp_rp = nullptr, *sp_ci = nullptr;
+    int *sp_flags = nullptr;
+    unsigned *sp_bar = nullptr;
+    double *sp_val = nullptr, *sp_dinv = nullptr, *sp_V = nullptr, *sp_z = nullptr,
+           *sp_w = nullptr, *sp_g = nullptr, *sp_x = nullptr, *sp_part = nullptr;
+    long long sp_solves = 0, sp_iters = 0, sp_fallbacks = 0;
+
     RunState rs;
     Prof prof;
 };
@@ -155,6 +165,16 @@ int factor32(Ctx &c);
 int coop_grid_size32(int n);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
+
+// ---- cutoff sparse path (d4_sparse.cu) ----
+bool gmres_selected(const Ctx &c);
+void sparse_alloc(Ctx &c);
+void sparse_free(Ctx &c);
+void sparse_prepare(Ctx &c);  // CSR of A (or A32); host-synchronising
+// GMRES solve of the stage; false when it did not converge (dense LU then).
+bool sparse_solve_update(Ctx &c, int gmode, double hval, const double *s_end,
+                         const double *s_init, const double *x_new, const double *x_old,
+                         const double *base, double *out);
 
 }  // namespace d4
 

@@ -113,6 +113,7 @@ class SimulationData:
         self.final_dislocation_configuration_path = ""
         self.logfile_path = ""
         self.precision_mode = _lib.D4_PREC_FP64
+        self.solver = _lib.D4_SOLVER_DENSE
         self.simulation_time = 0.0
         self.successful_steps = 0
         self.failed_steps = 0
@@ -165,6 +166,7 @@ class SimulationData:
         p.sub_config_times_type = self.sub_config_times_type.encode()[:1]
         p.protocol = self.external_stress.to_c()
         p.precision = self.precision_mode
+        p.solver = self.solver
         return p
 
 
@@ -267,6 +269,12 @@ class Engine:
         self._call("d4_profile_read", _lib.ptr(ms),
                    calls.ctypes.data_as(C.POINTER(C.c_longlong)))
         return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(_lib.CATEGORIES)}
+
+    def solver_stats(self):
+        """Counters of the cutoff sparse solver (d4_solver_stats)."""
+        v = [C.c_longlong() for _ in range(4)]
+        self._call("d4_solver_stats", *[C.byref(t) for t in v])
+        return dict(zip(("solves", "iterations", "fallbacks", "nnz"), [t.value for t in v]))
 
     def positions(self):
         x = np.empty(self.n)

@@ -50,6 +50,15 @@ enum {
     D4_PREC_MIXED = 1  /* FP32 pair sums + TF32 tensor-core LU + FP64 refinement */
 };
 
+/* Linear solver of the implicit step.  The reference factorises the (cutoff-
+   sparse) Jacobian with UMFPACK, src/simulation.cpp:635-659. */
+enum {
+    D4_SOLVER_DENSE = 0, /* dense LU (exact reference order in the FP64 form) */
+    D4_SOLVER_GMRES = 1, /* CSR of the cutoff Jacobian + Jacobi-preconditioned GMRES(40),
+                            relative residual 1e-13; dense LU when it does not converge */
+    D4_SOLVER_AUTO = 2   /* GMRES when the Jacobian's support radius^2 < 0.1, else dense */
+};
+
 /* External stress protocol (src/stress_protocol.cpp:13-73). */
 enum {
     D4_STRESS_NONE = 0,        /* StressProtocol: always 0 (even with tau0, as -s alone) */
@@ -91,6 +100,8 @@ typedef struct d4_params {
     int precision;                /* D4_PREC_FP64 or D4_PREC_MIXED (d4_set_matrix,
                                      d4_factor, d4_solve: FP64 form only) */
     int device;                   /* CUDA device ordinal */
+    int solver;                   /* D4_SOLVER_*: linear solver of the step (replaces the
+                                     UMFPACK calls of src/simulation.cpp:635-659) */
 } d4_params;
 
 /* Result of one attempted step (stages I-IV before acceptance). */
@@ -192,6 +203,14 @@ enum { D4_CAT_SPEEDS = 0, D4_CAT_JACOBIAN = 1, D4_CAT_FACTOR = 2, D4_CAT_SOLVE =
        D4_CAT_RESCALE = 4, D4_CAT_COUNT = 5 };
 int d4_profile(void *ctx, int enable);
 int d4_profile_read(void *ctx, double *ms, long long *calls);
+
+/* Counters of the cutoff sparse solver (D4_SOLVER_GMRES): GMRES solves run,
+ * Krylov iterations summed over them, solves that did not converge and were
+ * redone by the dense LU, and the entry count of the last CSR matrix.  No
+ * counterpart in the reference (UMFPACK's Info array is not read,
+ * src/simulation.cpp:637-645). */
+int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long long *fallbacks,
+                    long long *nnz);
 
 /* Number of kernels this library has launched in the process so far. */
 long long d4_kernel_launches(void);
