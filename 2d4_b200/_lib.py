@@ -14,6 +14,7 @@ D4_ERR = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "ba
           -5: "I/O error"}
 D4_PREC_FP64, D4_PREC_MIXED = 0, 1
 D4_SOLVER_DENSE, D4_SOLVER_GMRES, D4_SOLVER_AUTO = 0, 1, 2
+D4_FIELD_ANALYTIC, D4_FIELD_TABULATED = 0, 1
 D4_STRESS_NONE, D4_STRESS_FIXED_RATE, D4_STRESS_CYCLIC, D4_STRESS_INC_CYCLIC = 0, 1, 2, 3
 CATEGORIES = ["speeds", "jacobian", "factor", "solve", "rescale"]
 
@@ -35,7 +36,8 @@ class Params(C.Structure):
         ("save_sub_configs", C.c_int), ("sub_config_delay", C.c_uint),
         ("sub_config_delay_during_avalanche", C.c_uint), ("sub_config_times", C.c_double),
         ("sub_config_times_type", C.c_char), ("protocol", Protocol), ("precision", C.c_int),
-        ("device", C.c_int), ("solver", C.c_int)]
+        ("device", C.c_int), ("solver", C.c_int),
+        ("field", C.c_int), ("table_size", C.c_int)]
 
 
 class AttemptResult(C.Structure):

@@ -102,12 +102,14 @@ void free_all(Ctx *c) {
                     c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
                     c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red,
                     c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2,
+                    c->rowsub, c->rowsc,
                     c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
                     c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
                     c->m_w1, c->m_resid};
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
+    if (c->tab) cudaFree(c->tab);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_flags) cudaFreeHost(c->h_flags);
     for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
@@ -143,6 +145,26 @@ void download(Ctx &c, double *dst, const double *src) {
 }
 
 void sync(Ctx &c) { D4_CUDA_OK(cudaStreamSynchronize(c.stream)); }
+
+// Errors that kernels record instead of hanging (bounded waits), read back
+// into h_flags[0..5] from wave_err after a stream sync.
+void check_async_errors(Ctx &c) {
+    const int *werr = c.h_flags;
+    if (werr[0]) {
+        c.err_detail = "triangular solve wavefront timed out: block " + std::to_string(werr[1]) +
+                       " waiting for block " + std::to_string(werr[2]) + " saw flag " +
+                       std::to_string(werr[3]) + ", expected " + std::to_string(werr[4]);
+        throw d4::StateError(c.err_detail.c_str());
+    }
+    if (werr[d4::kWaveErrRows]) throw d4::StateError("row-sum pipeline wait timed out");
+}
+
+void read_async_errors(Ctx &c) {
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.wave_err, sizeof(int) * 6, cudaMemcpyDeviceToHost,
+                               c.stream));
+    sync(c);
+    check_async_errors(c);
+}
 
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
@@ -227,16 +249,11 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     d4::error_ratio64(c, c.xb, c.x2);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost,
                                c.stream));
-    int werr[5];
-    D4_CUDA_OK(cudaMemcpyAsync(werr, c.wave_err, sizeof(werr), cudaMemcpyDeviceToHost, c.stream));
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.wave_err, sizeof(int) * 6, cudaMemcpyDeviceToHost,
+                               c.stream));
     sync(c);
     if (c.prof.on) d4::prof_collect(c);
-    if (werr[0]) {
-        c.err_detail = "triangular solve wavefront timed out: block " + std::to_string(werr[1]) +
-                       " waiting for block " + std::to_string(werr[2]) + " saw flag " +
-                       std::to_string(werr[3]) + ", expected " + std::to_string(werr[4]);
-        throw d4::StateError(c.err_detail.c_str());
-    }
+    check_async_errors(c);
     const int idx = (int)c.h_red[1];
     if (idx >= 0) c.selected_id = idx;
     res->ratio = c.h_red[0] / c.dipole_prec_sq;
@@ -335,6 +352,8 @@ void d4_default_params(d4_params *p) {
     p->precision = D4_PREC_FP64;
     p->device = 0;
     p->solver = D4_SOLVER_DENSE;
+    p->field = D4_FIELD_ANALYTIC;
+    p->table_size = 1024;
 }
 
 int d4_create(void **out, int n, const d4_params *p) {
@@ -345,6 +364,10 @@ int d4_create(void **out, int n, const d4_params *p) {
         return D4_ERR_ARG;
     if (p->precision != D4_PREC_FP64 && p->precision != D4_PREC_MIXED) return D4_ERR_ARG;
     if (p->solver < D4_SOLVER_DENSE || p->solver > D4_SOLVER_AUTO) return D4_ERR_ARG;
+    if (p->field != D4_FIELD_ANALYTIC && p->field != D4_FIELD_TABULATED) return D4_ERR_ARG;
+    if (p->field == D4_FIELD_TABULATED &&
+        (p->precision != D4_PREC_FP64 || p->table_size < 16 || p->table_size > 4096))
+        return D4_ERR_ARG;
     Ctx *c = new (std::nothrow) Ctx();
     if (!c) return D4_ERR_NOMEM;
     try {
@@ -407,6 +430,8 @@ int d4_create(void **out, int n, const d4_params *p) {
         dalloc(&c->wave_err, 8);
         dalloc(&c->xw1, (size_t)n);
         dalloc(&c->xw2, (size_t)n);
+        dalloc(&c->rowsub, (size_t)n);
+        dalloc(&c->rowsc, (size_t)n);
         D4_CUDA_OK(cudaMemset(c->wave_done, 0, sizeof(unsigned) * nblk));
         D4_CUDA_OK(cudaMemset(c->wave_done2, 0, sizeof(unsigned) * nblk));
         D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int) * 8));
@@ -425,6 +450,10 @@ int d4_create(void **out, int n, const d4_params *p) {
         c->lu_mask_words = nblk * 33 + 8;
         dalloc(&c->lu_mask, (size_t)c->lu_mask_words);
         dalloc(&c->lu_bar, 64);
+        if (p->field == D4_FIELD_TABULATED) {
+            c->tab_T = p->table_size;
+            d4::table_build(*c);
+        }
         c->use_gmres = d4::gmres_selected(*c) ? 1 : 0;
         if (c->use_gmres) d4::sparse_alloc(*c);
         d4::reset_tol64(*c);
@@ -509,7 +538,7 @@ int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, doub
         d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
     download(*c, v, c->speed2);
     if (tol) download(*c, tol, c->tol);
-    sync(*c);
+    read_async_errors(*c);
     return D4_OK;
     D4_GUARD_END(c)
 }
@@ -533,7 +562,7 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
     if (dvec) download(*c, dvec, c->dvec);
     if (tol) download(*c, tol, c->tol);
     copy_matrix_out(*c, a_colmajor);
-    sync(*c);
+    read_async_errors(*c);
     return D4_OK;
     D4_GUARD_END(c)
 }

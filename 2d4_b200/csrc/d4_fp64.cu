@@ -16,8 +16,10 @@
 #include <cstdint>
 #include <mutex>
 
+#include "d4_bulk.cuh"
 #include "d4_field64.cuh"
 #include "d4_internal.h"
+#include "d4_table.cuh"
 
 namespace d4 {
 namespace {
@@ -53,11 +55,13 @@ struct PairArgs {
     double h;       // step size of the Jacobian
     double cut_sq, cutoff, range_sq, one_per_cut_sq;
     int heaviside;
+    tab::Table tb;  // tabulated field (kTab kernels only)
 };
 
 // One 32x32 tile of pairs per block; threadIdx.x = local i (coalesced column
-// stores), threadIdx.y steps local j.
-template <bool kJac>
+// stores), threadIdx.y steps local j.  kTab: the field and its x-derivative come
+// from the table (d4_table.cuh) instead of the analytic image sums.
+template <bool kJac, bool kTab = false>
 __global__ void __launch_bounds__(256) k_pairs64(PairArgs a) {
     const int T = (a.n + kTile - 1) / kTile;
     int ti, tj;
@@ -90,12 +94,21 @@ __global__ void __launch_bounds__(256) k_pairs64(PairArgs a) {
                 tol_min(a.tol, j, dist_sq);
             }
             const double bj = bsign(j, a.n);
-            f64::Hyp hp(f64::exp2pix(dx));
-            double c = f64::cos2piy(dy);
-            f = f64::xy(dx, dy, hp, c) * bi * bj;
+            double fxy, fdx = 0;
+            if (kTab) {
+                const double2 t = tab::eval<kJac>(a.tb, dx, dy);
+                fxy = t.x;
+                fdx = t.y;
+            } else {
+                f64::Hyp hp(f64::exp2pix(dx));
+                double c = f64::cos2piy(dy);
+                fxy = f64::xy(dx, dy, hp, c);
+                if (kJac && dist_sq < a.range_sq * a.cut_sq) fdx = f64::xy_diff_x(dx, dy, hp, c);
+            }
+            f = fxy * bi * bj;
             if (kJac) {
                 if (dist_sq < a.range_sq * a.cut_sq) {
-                    v = a.h * bj * bi * f64::xy_diff_x(dx, dy, hp, c);
+                    v = a.h * bj * bi * fdx;
                     if (!a.heaviside && dist_sq > a.cut_sq) {
                         double t = sqrt(dist_sq) - a.cutoff;
                         v *= exp(-(t * t) * a.one_per_cut_sq);
@@ -142,47 +155,129 @@ __global__ void k_rows_speed64(int n, const double *__restrict__ F, double ext, 
     v[i] = s + ext * bsign(i, n);
 }
 
-// Ordered row sums of the fused sweep and the row scaling
-// (src/simulation.cpp:503-522): A[i,i] = subSum, d_i = weight(subSum),
-// row i scaled by (1 + d_i)/2, +1 on the diagonal.
-__global__ void k_rows_jac64(int n, const double *__restrict__ F, double *A, double ext_a,
-                             double ext_b, double *v_a, double *v_b, double *dvec, char wfn) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double s = 0, sub = 0;
-    int j = 0;
-    for (; j + 8 <= n; j += 8) {
-        double tf[8], ta[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            tf[u] = __ldg(F + (size_t)i + (size_t)(j + u) * n);
-            ta[u] = A[(size_t)i + (size_t)(j + u) * n];
+// Ordered row sums, pipelined.  Block b owns rows i0 = 32 b .. i0 + 31; F (and,
+// in the fused sweep, the raw Jacobian A) are column-major, so the 32 rows of
+// one column are 256 contiguous bytes.  Warp 1 streams them column chunk by
+// column chunk into shared memory with bulk copies (kRowStages chunks of
+// kRowCols columns in flight, each completing on its stage's mbarrier); warp 0
+// has one lane per row and adds the entries in ascending j, exactly the
+// reference's summation order (src/simulation.cpp:292-311,444-503).  The fused
+// sweep then writes subSum, d_i = weight(subSum) and the row scale (1 + d_i)/2
+// for k_scale_rows64.  A wait that gives up records err[0] = 1 and the block
+// drains its copies in flight before it returns.
+constexpr int kRowRows = 32, kRowCols = 64, kRowStages = 4;
+
+struct RowArgs {
+    int n;
+    const double *F, *A;
+    double ext_a, ext_b;
+    double *v_a, *v_b;  // stress sweep: v_a only
+    double *dvec, *rowsub, *rowsc;
+    char wfn;
+    int *err;
+};
+
+template <bool kJac>
+constexpr int row_smem_bytes() {
+    return (kJac ? 2 : 1) * kRowStages * kRowCols * kRowRows * (int)sizeof(double);
+}
+
+template <bool kJac>
+__global__ void __launch_bounds__(64) k_rows64(RowArgs a) {
+    extern __shared__ __align__(128) unsigned char row_smem[];
+    double *bf = reinterpret_cast<double *>(row_smem);  // [stage][col][row]
+    double *ba = bf + kRowStages * kRowCols * kRowRows;
+    __shared__ __align__(8) uint64_t full[kRowStages], empty[kRowStages];
+    __shared__ int issued_s, consumed_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = a.n;
+    const int i0 = blockIdx.x * kRowRows;
+    const int rows = min(kRowRows, n - i0);
+    const int nst = (n + kRowCols - 1) / kRowCols;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kRowStages; ++s) {
+            bulk::init(&full[s], 1);
+            bulk::init(&empty[s], 1);
         }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-            if (j + u != i) {
-                s += tf[u];
-                sub -= ta[u];
+        bulk::fence_init();
+        issued_s = 0;
+        consumed_s = 0;
+    }
+    __syncthreads();
+    if (warp == 1) {
+        // producer
+        const uint32_t col_bytes = rows * (uint32_t)sizeof(double);
+        int st = 0;
+        for (; st < nst; ++st) {
+            const int s = st % kRowStages;
+            const uint32_t use = st / kRowStages;
+            if (use > 0 && !__all_sync(0xffffffffu, bulk::wait(&empty[s], (use - 1) & 1))) {
+                if (lane == 0) atomicOr(a.err, 1);
+                break;
             }
+            const int j0 = st * kRowCols, nc = min(kRowCols, n - j0);
+            if (lane == 0) bulk::arrive_expect_tx(&full[s], nc * col_bytes * (kJac ? 2 : 1));
+            __syncwarp();
+            for (int k = lane; k < nc; k += 32) {
+                const size_t off = (size_t)i0 + (size_t)(j0 + k) * n;
+                const int slot = (s * kRowCols + k) * kRowRows;
+                bulk::g2s(bf + slot, a.F + off, col_bytes, &full[s]);
+                if (kJac) bulk::g2s(ba + slot, a.A + off, col_bytes, &full[s]);
+            }
+        }
+        if (lane == 0) issued_s = st;
+    } else {
+        // consumer: lane = row
+        const int i = i0 + lane;
+        double sum = 0, sub = 0;
+        int st = 0;
+        for (; st < nst; ++st) {
+            const int s = st % kRowStages;
+            if (!__all_sync(0xffffffffu, bulk::wait(&full[s], (st / kRowStages) & 1))) {
+                if (lane == 0) atomicOr(a.err, 1);
+                break;
+            }
+            const int j0 = st * kRowCols, nc = min(kRowCols, n - j0);
+            const double *cf = bf + s * kRowCols * kRowRows + lane;
+            const double *ca = ba + s * kRowCols * kRowRows + lane;
+            for (int k = 0; k < nc; ++k) {
+                if (j0 + k == i) continue;
+                sum += cf[k * kRowRows];
+                if (kJac) sub -= ca[k * kRowRows];
+            }
+            __syncwarp();
+            if (lane == 0) bulk::arrive(&empty[s]);
+        }
+        if (lane == 0) consumed_s = st;
+        if (st == nst && lane < rows) {
+            const double b = bsign(i, n);
+            if (kJac) {
+                a.v_b[i] = sum + a.ext_b * b;
+                a.v_a[i] = sum + a.ext_a * b;
+                const double d = f64::weight(sub, a.wfn);
+                a.dvec[i] = d;
+                a.rowsub[i] = sub;
+                a.rowsc[i] = (1 + d) / 2;
+            } else {
+                a.v_a[i] = sum + a.ext_a * b;
+            }
+        }
     }
-    for (; j < n; ++j) {
-        if (j == i) continue;
-        s += F[(size_t)i + (size_t)j * n];
-        sub -= A[(size_t)i + (size_t)j * n];
-    }
-    const double b = bsign(i, n);
-    v_b[i] = s + ext_b * b;
-    v_a[i] = s + ext_a * b;
-    const double d = f64::weight(sub, wfn);
-    dvec[i] = d;
-    const double sc = (1 + d) / 2;
-    for (j = 0; j < n; ++j) {
-        double *e = A + (size_t)i + (size_t)j * n;
-        if (j == i)
-            *e = sub * sc + 1;
-        else
-            *e = *e * sc;
-    }
+    __syncthreads();
+    // after a failed wait: let the copies in flight land before the block exits
+    if (threadIdx.x == 32)
+        for (int st = consumed_s; st < issued_s; ++st)
+            bulk::wait(&full[st % kRowStages], (st / kRowStages) & 1);
+}
+
+// Row scaling of the fused sweep (src/simulation.cpp:516-522): A[i,i] =
+// subSum_i * sc_i + 1, A[i,j] *= sc_i otherwise (coalesced, column-major).
+__global__ void k_scale_rows64(int n, double *A, const double *rowsub, const double *rowsc) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)n * n) return;
+    const int r = (int)(idx % n), c = (int)(idx / n);
+    const double sc = rowsc[r];
+    A[idx] = (r == c) ? rowsub[r] * sc + 1 : A[idx] * sc;
 }
 
 // calcJacobianAndSpeedsFromPrev weights (src/simulation.cpp:552-582).
@@ -282,6 +377,16 @@ __global__ void k_strain64(int n, const double *old, const double *nw, double *o
     *out = r;
 }
 
+// The tabulated field at given points.
+__global__ void k_field_tab64(tab::Table tb, int count, const double *dx, const double *dy,
+                              double *xy, double *xyd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const double2 t = tab::eval<true>(tb, dx[k], dy[k]);
+    xy[k] = t.x;
+    xyd[k] = t.y;
+}
+
 // Field::xy (2-arg, exp2) and Field::xy_diff_x (2-arg, exp) at given points.
 __global__ void k_field64(int count, const double *dx, const double *dy, double *xy,
                           double *xyd) {
@@ -314,7 +419,19 @@ static PairArgs pair_args(Ctx &c, const double *x, const double *y) {
     a.range_sq = c.range_sq;
     a.one_per_cut_sq = 1 / c.cutoff_sq;
     a.heaviside = c.p.heaviside_cutoff;
+    a.tb.t = c.tab;
+    a.tb.T = c.tab_T;
+    a.tb.W = c.tab_T + 1 + 2 * tab::kGuard;
     return a;
+}
+
+template <bool kJac>
+static void launch_rows(Ctx &c, const RowArgs &r) {
+    constexpr int bytes = row_smem_bytes<kJac>();
+    D4_CUDA_OK(cudaFuncSetAttribute(k_rows64<kJac>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    bytes));
+    k_rows64<kJac><<<(c.n + kRowRows - 1) / kRowRows, 64, bytes, c.stream>>>(r);
+    check_launch(kJac ? "k_rows64<jacobian>" : "k_rows64<speeds>");
 }
 
 static int pair_blocks(int n) {
@@ -324,21 +441,46 @@ static int pair_blocks(int n) {
 
 void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v) {
     PairArgs a = pair_args(c, x, y);
-    k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    if (c.tab)
+        k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    else
+        k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
     check_launch("k_pairs64<speeds>");
-    k_rows_speed64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.F, ext, v);
-    check_launch("k_rows_speed64");
+    RowArgs r{};
+    r.n = c.n;
+    r.F = c.F;
+    r.ext_a = ext;
+    r.v_a = v;
+    r.err = c.wave_err + kWaveErrRows;
+    launch_rows<false>(c, r);
 }
 
 void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
                 double *v_a, double *v_b) {
     PairArgs a = pair_args(c, x, y);
     a.h = h;
-    k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    if (c.tab)
+        k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+    else
+        k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
     check_launch("k_pairs64<jacobian>");
-    k_rows_jac64<<<blocks(c.n, 128), 128, 0, c.stream>>>(c.n, c.F, c.A, ext_a, ext_b, v_a, v_b,
-                                                         c.dvec, c.p.weight_function);
-    check_launch("k_rows_jac64");
+    RowArgs r{};
+    r.n = c.n;
+    r.F = c.F;
+    r.A = c.A;
+    r.ext_a = ext_a;
+    r.ext_b = ext_b;
+    r.v_a = v_a;
+    r.v_b = v_b;
+    r.dvec = c.dvec;
+    r.rowsub = c.rowsub;
+    r.rowsc = c.rowsc;
+    r.wfn = c.p.weight_function;
+    r.err = c.wave_err + kWaveErrRows;
+    launch_rows<true>(c, r);
+    k_scale_rows64<<<blocks((long long)c.n * c.n, 256), 256, 0, c.stream>>>(c.n, c.A, c.rowsub,
+                                                                           c.rowsc);
+    check_launch("k_scale_rows64");
 }
 
 void jacobian_from_prev64(Ctx &c, double factor) {
@@ -387,6 +529,12 @@ void strain_increment64(Ctx &c, const double *x_old, const double *x_new, double
 
 void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double *xy,
                   double *xyd) {
+    if (c.tab) {
+        PairArgs a = pair_args(c, nullptr, nullptr);
+        k_field_tab64<<<blocks(count, 128), 128, 0, c.stream>>>(a.tb, count, dx, dy, xy, xyd);
+        check_launch("k_field_tab64");
+        return;
+    }
     k_field64<<<blocks(count, 128), 128, 0, c.stream>>>(count, dx, dy, xy, xyd);
     check_launch("k_field64");
 }

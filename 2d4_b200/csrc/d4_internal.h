@@ -25,6 +25,10 @@ enum FlagSlot {
     kFlagCount = 8
 };
 
+// wave_err words: [0..4] wavefront-solve diagnostics, [5] a row-sum pipeline
+// wait gave up.
+constexpr int kWaveErrRows = 5;
+
 // State of Simulation::run's loop kept between d4_advance calls.
 struct RunState {
     bool started = false;
@@ -84,6 +88,8 @@ struct Ctx {
     unsigned wave_epoch = 0;
     int *wave_err = nullptr;
     double *xw1 = nullptr, *xw2 = nullptr;
+    // row sums of the FP64 fused sweep: subSum_i and the row scale (1 + d_i)/2
+    double *rowsub = nullptr, *rowsc = nullptr;
     // cooperative LU: saved block columns, pre-division values, per-pass masks,
     // grid barrier words
     double *lu_p0 = nullptr, *lu_q = nullptr;
@@ -109,6 +115,10 @@ struct Ctx {
     double *sp_val = nullptr, *sp_dinv = nullptr, *sp_V = nullptr, *sp_z = nullptr,
            *sp_w = nullptr, *sp_g = nullptr, *sp_x = nullptr, *sp_part = nullptr;
     long long sp_solves = 0, sp_iters = 0, sp_fallbacks = 0;
+
+    // tabulated field (null: analytic field)
+    double2 *tab = nullptr;
+    int tab_T = 0;
 
     RunState rs;
     Prof prof;
@@ -165,6 +175,9 @@ int factor32(Ctx &c);
 int coop_grid_size32(int n);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
+
+// ---- tabulated field (d4_table.cu) ----
+void table_build(Ctx &c);  // allocates c.tab (T = c.tab_T) and fills it on c.stream
 
 // ---- cutoff sparse path (d4_sparse.cu) ----
 bool gmres_selected(const Ctx &c);

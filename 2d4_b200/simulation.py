@@ -114,6 +114,8 @@ class SimulationData:
         self.logfile_path = ""
         self.precision_mode = _lib.D4_PREC_FP64
         self.solver = _lib.D4_SOLVER_DENSE
+        self.field = _lib.D4_FIELD_ANALYTIC
+        self.table_size = 1024
         self.simulation_time = 0.0
         self.successful_steps = 0
         self.failed_steps = 0
@@ -167,6 +169,8 @@ class SimulationData:
         p.protocol = self.external_stress.to_c()
         p.precision = self.precision_mode
         p.solver = self.solver
+        p.field = self.field
+        p.table_size = self.table_size
         return p
 
 
@@ -334,13 +338,17 @@ class Simulation:
 
 class Field:
     """Field::xy / Field::xy_diff_x (src/Fields/Field.cpp:333-346) evaluated on
-    the device in FP64."""
+    the device in FP64; with tabulated=True, the tabulated field
+    (PeriodicShearStressELTE's role, table_size intervals per axis)."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, tabulated=False, table_size=1024):
         self.lib = _lib.load()
         p = _lib.Params()
         self.lib.d4_default_params(C.byref(p))
         p.device = device
+        if tabulated:
+            p.field = _lib.D4_FIELD_TABULATED
+            p.table_size = table_size
         ctx = C.c_void_p()
         _lib.check(self.lib, None, self.lib.d4_create(C.byref(ctx), 2, C.byref(p)), "d4_create")
         self.ctx = ctx

@@ -59,6 +59,18 @@ enum {
     D4_SOLVER_AUTO = 2   /* GMRES when the Jacobian's support radius^2 < 0.1, else dense */
 };
 
+/* Field of a pair.  The reference's core uses the analytic image sum
+   (src/Fields/Field.cpp:172-346); its Python binding also names a tabulated
+   field (PeriodicShearStressELTE, python/src/periodic_shear_stress_ELTE_wrapper.cpp:43-44)
+   whose tables are not part of the reference. */
+enum {
+    D4_FIELD_ANALYTIC = 0,  /* Field::xy / Field::xy_diff_x */
+    D4_FIELD_TABULATED = 1  /* table of the smooth remainder after the free-space
+                               core on a table_size^2 grid, bicubic (four-point
+                               Lagrange) interpolation + the analytic core;
+                               FP64 form only */
+};
+
 /* External stress protocol (src/stress_protocol.cpp:13-73). */
 enum {
     D4_STRESS_NONE = 0,        /* StressProtocol: always 0 (even with tau0, as -s alone) */
@@ -102,6 +114,9 @@ typedef struct d4_params {
     int device;                   /* CUDA device ordinal */
     int solver;                   /* D4_SOLVER_*: linear solver of the step (replaces the
                                      UMFPACK calls of src/simulation.cpp:635-659) */
+    int field;                    /* D4_FIELD_*, default analytic */
+    int table_size;               /* intervals per axis of the tabulated field, default
+                                     1024 (loadStress(..., 1024)); 16..4096 */
 } d4_params;
 
 /* Result of one attempted step (stages I-IV before acceptance). */
@@ -235,7 +250,8 @@ long long d4_kernel_launches(void);
 int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress, double *v,
                       double *tol, double min_prec_sq, void *stream);
 
-/* Single field evaluations on the device (FP64 path), for checks. */
+/* Single field evaluations on the device, for checks: the context's field
+ * (analytic FP64 Field::xy / Field::xy_diff_x, or the tabulated field). */
 int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
                   double *xy_diff_x);
 
