@@ -48,6 +48,18 @@ def test_default_params_and_bad_arguments(pkg):
     p.weight_function = b"x"
     assert lib.d4_create(C.byref(ctx), 64, C.byref(p)) == -1
     assert lib.d4_destroy(None) == -1
+    # solver and field selection: defaults, and combinations rejected before any
+    # device work (unknown solver, tabulated field in the mixed form, table size)
+    lib.d4_default_params(C.byref(p))
+    assert p.solver == pkg._lib.D4_SOLVER_DENSE and p.field == pkg._lib.D4_FIELD_ANALYTIC
+    assert p.table_size == 1024
+    for kw in (dict(solver=7), dict(field=2),
+               dict(field=1, precision=pkg._lib.D4_PREC_MIXED),
+               dict(field=1, table_size=8), dict(field=1, table_size=8192)):
+        lib.d4_default_params(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        assert lib.d4_create(C.byref(ctx), 64, C.byref(p)) == -1, kw
 
 
 def test_dconf_roundtrip_and_sort(pkg, golden, tmp_path):
