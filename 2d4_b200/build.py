@@ -1,4 +1,4 @@
-"""Builds libd4core.so (sm_100a) in-tree with nvcc.
+"""Builds libd4core.so (sm_100a) and libd4umfpack.so in-tree.
 
 Usage: python 2d4_b200/build.py [--jobs N]
 
@@ -6,7 +6,9 @@ Each .cu file under csrc/ compiles to an object with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the FP64 files of
 the plain form add ``--fmad=false`` so that no product-add is contracted into
 an FMA (they keep the reference's rounding of every operation).  The objects
-link into ``2d4_b200/lib/libd4core.so``.
+link into ``2d4_b200/lib/libd4core.so``.  ``umfpack/d4_umfpack.cpp`` (host
+C++) links against it into ``2d4_b200/lib/libd4umfpack.so``, the
+UMFPACK-compatible entry points, with an ``$ORIGIN`` run path.
 """
 import os
 import subprocess
@@ -19,6 +21,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 BUILD_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libd4core.so")
+UMF_SRC = os.path.join(HERE, "umfpack", "d4_umfpack.cpp")
+UMF_LIB = os.path.join(OUT_DIR, "libd4umfpack.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -60,13 +64,27 @@ def build(jobs=8):
     os.makedirs(BUILD_DIR, exist_ok=True)
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(compile_one, sources()))
-    if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if not (os.path.exists(LIB) and
+            all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs)):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    build_umfpack()
+    return LIB
+
+
+def build_umfpack():
+    deps = [UMF_SRC, LIB, os.path.join(ROOT, "include", "d4umfpack.h")]
+    if os.path.exists(UMF_LIB) and all(os.path.getmtime(UMF_LIB) >= os.path.getmtime(d)
+                                       for d in deps):
+        return UMF_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"),
+           "-o", UMF_LIB, UMF_SRC, "-L" + OUT_DIR, "-ld4core", "-Wl,-rpath,$ORIGIN"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
-    return LIB
+        raise RuntimeError("g++ failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    return UMF_LIB
 
 
 if __name__ == "__main__":
