@@ -5,10 +5,11 @@ The package is named ``2d4_b200``; import it with
 (hand-written sm_100a CUDA behind the C ABI of include/d4core.h).
 """
 from . import _lib, dconf
+from .ensemble import Ensemble
 from .simulation import (CyclicLoadProtocol, Engine, Field, FixedRateProtocol,
                          FixedRateStressProtocolObject, IncreasingCyclicLoadProtocol, Simulation,
                          SimulationData, StressProtocol, StressProtocolObject)
 
-__all__ = ["_lib", "dconf", "Engine", "Field", "Simulation", "SimulationData", "StressProtocol",
+__all__ = ["_lib", "dconf", "Engine", "Ensemble", "Field", "Simulation", "SimulationData", "StressProtocol",
            "StressProtocolObject", "FixedRateProtocol", "FixedRateStressProtocolObject",
            "CyclicLoadProtocol", "IncreasingCyclicLoadProtocol"]

@@ -87,6 +87,13 @@ SIGNATURES = {
     "d4_profile_read": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)]),
     "d4_kernel_launches": (C.c_longlong, []),
     "d4_solver_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 4),
+    "d4_ensemble_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(Params)]),
+    "d4_ensemble_destroy": (C.c_int, [_vp]),
+    "d4_ensemble_last_error": (C.c_char_p, [_vp]),
+    "d4_ensemble_set_positions": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "d4_ensemble_get_positions": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "d4_ensemble_run": (C.c_int, [_vp, C.c_longlong, C.POINTER(RunResult)]),
     "d4_speeds_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
                                     C.c_void_p, C.c_double, C.c_void_p]),
 }

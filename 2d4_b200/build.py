@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 # Files whose arithmetic must round like the reference's IEEE build.
-NO_FMA = {"d4_fp64.cu", "d4_lu64.cu", "d4_lu_coop64.cu"}
+NO_FMA = {"d4_fp64.cu", "d4_lu64.cu", "d4_lu_coop64.cu", "d4_ensemble.cu"}
 
 
 def nvcc():

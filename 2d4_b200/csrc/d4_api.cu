@@ -55,12 +55,9 @@ void prof_collect(Ctx &c) {
     }
     c.prof.used = 0;
 }
-}  // namespace d4
-
-namespace {
 
 // StressProtocol family, src/stress_protocol.cpp:13-73.
-double ext_stress(const d4_protocol &p, double t) {
+double ext_stress_host(const d4_protocol &p, double t) {
     switch (p.kind) {
     case D4_STRESS_FIXED_RATE:
         return t * p.rate + p.tau0;
@@ -76,6 +73,11 @@ double ext_stress(const d4_protocol &p, double t) {
         return 0;
     }
 }
+}  // namespace d4
+
+namespace {
+
+inline double ext_stress(const d4_protocol &p, double t) { return d4::ext_stress_host(p, t); }
 
 // SimulationData::getNextWriteOutTime, src/simulation_data.cpp:231-246.
 double next_write_out(const d4_params &p, double sim_time) {

@@ -176,6 +176,9 @@ int coop_grid_size32(int n);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
 
+// tau_ext(t) of the stress protocol (d4_api.cu).
+double ext_stress_host(const d4_protocol &p, double t);
+
 // ---- tabulated field (d4_table.cu) ----
 void table_build(Ctx &c);  // allocates c.tab (T = c.tab_T) and fills it on c.stream
 

@@ -227,6 +227,30 @@ int d4_profile_read(void *ctx, double *ms, long long *calls);
 int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long long *fallbacks,
                     long long *nnz);
 
+/* Batched ensemble of independent systems: the many-realisation statistics
+ * workload, where the reference runs one system per process
+ * (src/simulation.cpp:30-281).  FP64 form, analytic field, dense LU; every
+ * instance shares the parameters p (protocol, precisions, limits, cutoff
+ * multiplier) and instance k has n[k] dislocations (even, 2..8192, internal
+ * order).  Each attempt round runs stages I-IV for every active instance with
+ * one launch per phase (all instances' pair tiles and row blocks in one grid;
+ * one CTA per instance for an exact-order LU and the substitutions, so each
+ * instance reproduces d4_run's arithmetic), then applies each instance's step
+ * control as d4_run does (src/simulation.cpp:88-277; no log, sub-configuration
+ * or write-out clipping).  An instance stays active until interrupt() holds
+ * (time, strain or step-count limit, src/simulation.cpp:722-750). */
+int d4_ensemble_create(void **ens, int count, const int *n, const d4_params *p);
+int d4_ensemble_destroy(void *ens);
+const char *d4_ensemble_last_error(void *ens);
+int d4_ensemble_set_positions(void *ens, int k, const double *x, const double *y);
+int d4_ensemble_get_positions(void *ens, int k, double *x, double *y);
+/* Runs attempt rounds until no instance is active or max_rounds rounds
+ * (<= 0: no cap) have run in this call; may be called again to continue.
+ * res[count] receives each instance's totals (sim_time, step_size, strain,
+ * successful and failed steps, attempts, singular factorisations) and, in
+ * every entry, device_seconds = the CUDA-event span of this call. */
+int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res);
+
 /* Number of kernels this library has launched in the process so far. */
 long long d4_kernel_launches(void);
 
