@@ -87,6 +87,14 @@ SIGNATURES = {
     "d4_profile_read": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)]),
     "d4_kernel_launches": (C.c_longlong, []),
     "d4_solver_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 4),
+    "d4_record_steps": (C.c_int, [_vp, C.c_int]),
+    "d4_recorded_count": (C.c_longlong, [_vp]),
+    "d4_recorded_steps": (C.c_int, [_vp, C.c_longlong, _dp, _dp]),
+    "d4_replay": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(Protocol), _dp, _dp, _dp]),
+    "d4_tangent": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(Protocol), _dp, _dp,
+                             C.c_double, _dp, _dp]),
+    "d4_adjoint": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(Protocol), C.c_int, _dp,
+                             _dp, _dp, _dp]),
     "d4_ensemble_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(Params)]),
     "d4_ensemble_destroy": (C.c_int, [_vp]),

@@ -687,6 +687,10 @@ static int run_loop(Ctx *c, const d4_run_io *io, std::ofstream *log, long long t
         rs.pivoted += ar.pivoted;
         rs.singular += ar.singular;
         if (ar.ratio < 1) {
+            if (c->recording) {
+                c->rec_t0.push_back(c->sim_time);
+                c->rec_h.push_back(h);
+            }
             c->sim_time += h;
             ++rs.ok;
             if (p.calculate_strain) {
@@ -890,6 +894,33 @@ int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long lo
     *iterations = c->sp_iters;
     *fallbacks = c->sp_fallbacks;
     *nnz = c->sp_nnz;
+    return D4_OK;
+}
+
+int d4_record_steps(void *ctx, int enable) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    if (enable) {
+        c->rec_t0.clear();
+        c->rec_h.clear();
+    }
+    c->recording = enable != 0;
+    return D4_OK;
+}
+
+long long d4_recorded_count(void *ctx) {
+    Ctx *c = (Ctx *)ctx;
+    return c ? (long long)c->rec_t0.size() : -1;
+}
+
+int d4_recorded_steps(void *ctx, long long count, double *t0s, double *hs) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || count < 0 || (count > 0 && (!t0s || !hs))) return D4_ERR_ARG;
+    const long long m = std::min<long long>(count, (long long)c->rec_t0.size());
+    for (long long k = 0; k < m; ++k) {
+        t0s[k] = c->rec_t0[k];
+        hs[k] = c->rec_h[k];
+    }
     return D4_OK;
 }
 

@@ -120,6 +120,10 @@ struct Ctx {
     double2 *tab = nullptr;
     int tab_T = 0;
 
+    // accepted steps (t0, h) recorded by the run loop (d4_record_steps)
+    bool recording = false;
+    std::vector<double> rec_t0, rec_h;
+
     RunState rs;
     Prof prof;
 };

@@ -264,6 +264,63 @@ class Engine:
         self._call("d4_advance", C.c_longlong(accepted_steps), C.byref(r))
         return r
 
+    # accepted-step recording and the differentiation of a replayed step sequence
+    def record_steps(self, enable=True):
+        self._call("d4_record_steps", int(bool(enable)))
+
+    def recorded_steps(self):
+        """(t0s, hs) of the accepted steps recorded since record_steps(True)."""
+        m = self.lib.d4_recorded_count(self.ctx)
+        t0s, hs = np.empty(max(m, 0)), np.empty(max(m, 0))
+        self._call("d4_recorded_steps", C.c_longlong(m), _lib.ptr(t0s), _lib.ptr(hs))
+        return t0s, hs
+
+    @staticmethod
+    def _steps(t0s, hs):
+        t0s = np.ascontiguousarray(t0s, dtype=np.float64)
+        hs = np.ascontiguousarray(hs, dtype=np.float64)
+        assert t0s.shape == hs.shape
+        return t0s, hs
+
+    def _proto(self, tau0):
+        p = self.sd.external_stress.to_c()
+        if tau0 is not None:
+            p.tau0 = float(tau0)
+        return p
+
+    def replay(self, x0, t0s, hs, tau0=None):
+        """Strain and final positions of the fixed-step replay (d4_replay)."""
+        t0s, hs = self._steps(t0s, hs)
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        x_end, strain = np.empty(self.n), C.c_double()
+        p = self._proto(tau0)
+        self._call("d4_replay", C.c_longlong(len(t0s)), _lib.ptr(t0s), _lib.ptr(hs), C.byref(p),
+                   _lib.ptr(x0), _lib.ptr(x_end), C.byref(strain))
+        return strain.value, x_end
+
+    def tangent(self, x0, t0s, hs, dx0, dtau0=0.0, tau0=None):
+        """(strain, directional derivative along (dx0, dtau0)) (d4_tangent)."""
+        t0s, hs = self._steps(t0s, hs)
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        dx0 = np.ascontiguousarray(dx0, dtype=np.float64)
+        strain, ds = C.c_double(), C.c_double()
+        p = self._proto(tau0)
+        self._call("d4_tangent", C.c_longlong(len(t0s)), _lib.ptr(t0s), _lib.ptr(hs),
+                   C.byref(p), _lib.ptr(x0), _lib.ptr(dx0), C.c_double(dtau0), C.byref(strain),
+                   C.byref(ds))
+        return strain.value, ds.value
+
+    def adjoint(self, x0, t0s, hs, checkpoint_every=20, tau0=None):
+        """(strain, d strain / d x0, d strain / d tau0) (d4_adjoint)."""
+        t0s, hs = self._steps(t0s, hs)
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        g, strain, gt = np.empty(self.n), C.c_double(), C.c_double()
+        p = self._proto(tau0)
+        self._call("d4_adjoint", C.c_longlong(len(t0s)), _lib.ptr(t0s), _lib.ptr(hs),
+                   C.byref(p), int(checkpoint_every), _lib.ptr(x0), C.byref(strain), _lib.ptr(g),
+                   C.byref(gt))
+        return strain.value, g, gt.value
+
     def profile(self, enable=True):
         self._call("d4_profile", int(bool(enable)))
 

@@ -251,6 +251,39 @@ int d4_ensemble_get_positions(void *ens, int k, double *x, double *y);
  * every entry, device_seconds = the CUDA-event span of this call. */
 int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res);
 
+/* Recording of accepted steps: while enabled, d4_run and d4_advance append
+ * each accepted step's start time and size (the t and h of
+ * src/simulation.cpp:88-164) to the context's list.  enable = 1 clears the
+ * list and starts, 0 stops.  d4_recorded_steps copies up to `count` entries. */
+int d4_record_steps(void *ctx, int enable);
+long long d4_recorded_count(void *ctx);
+int d4_recorded_steps(void *ctx, long long count, double *t0s, double *hs);
+
+/* Differentiation of a fixed sequence of accepted steps (no counterpart in the
+ * reference).  The forward map replays steps (t0s[k], hs[k]) from positions
+ * x0 (internal order, the context's y): the stages II and III of
+ * Simulation::run's attempt (src/simulation.cpp:115-150) with the engine's
+ * FP64 kernels, then normalize; the loss is the accumulated strain
+ * sum_k sum_i b_i (x2_i - x0_i) (src/simulation.cpp:713-720).  Step sizes are
+ * constants.  proto may be null (the context's protocol); tau0 is its tau0.
+ * FP64 form, analytic field, dense solver, no cutoff; the context's positions
+ * and tolerances are left as they were.
+ *   d4_replay   strain and final positions (x_end may be null)
+ *   d4_tangent  strain and its directional derivative along (dx0, dtau0)
+ *   d4_adjoint  strain, d strain / d x0 and d strain / d tau0, with positions
+ *               checkpointed every checkpoint_every steps, each segment
+ *               recomputed in the backward sweep and the step's LU factors
+ *               reused for the transposed solves (device memory: about
+ *               2 checkpoint_every n^2 doubles for the segment's factors). */
+int d4_replay(void *ctx, long long steps, const double *t0s, const double *hs,
+              const d4_protocol *proto, const double *x0, double *x_end, double *strain);
+int d4_tangent(void *ctx, long long steps, const double *t0s, const double *hs,
+               const d4_protocol *proto, const double *x0, const double *dx0, double dtau0,
+               double *strain, double *dstrain);
+int d4_adjoint(void *ctx, long long steps, const double *t0s, const double *hs,
+               const d4_protocol *proto, int checkpoint_every, const double *x0, double *strain,
+               double *grad_x0, double *grad_tau0);
+
 /* Number of kernels this library has launched in the process so far. */
 long long d4_kernel_launches(void);
 
