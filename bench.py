@@ -2,7 +2,8 @@
 """Throughput of the 2D4_sim implicit step on B200: dislocation-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c3-fp64] [--no-cpu-baseline]
+                    [--workload c2|c1|c3-fp64] [--no-cpu-baseline] [--no-mixed]
+                    [--legs cutoff,tabulated,ensemble,adjoint|none]
 
 A step is one ACCEPTED implicit step (stages I-IV of src/simulation.cpp:88-277;
 the failed attempts between accepted steps are part of its cost).  The metric is
@@ -26,6 +27,11 @@ N / that time.
 --impl reference: the reference core built from its own sources with its own
 flags (oracle/_ref/libd4ref_fast.so, UMFPACK replaced by OpenBLAS dgetrf/dgetrs on
 all host cores) on the same workload, through Simulation::run, rank 0 only.
+
+At N=1 the line also carries bounded legs for the other configurations:
+mixed_vs_fp64 (N=4096 dense), cutoff (N=4096, Heaviside c = 0.1: FP64 dense,
+FP64 GMRES, mixed GMRES), tabulated (the N=1024 workload with the tabulated
+field), ensemble (512 instances of uneven N) and adjoint (N=2048, 200 steps).
 """
 import argparse
 import glob
@@ -257,6 +263,133 @@ def mixed_vs_fp64(pkg, steps=8, warmup=2, n=4096, seed=1002, tau=0.1):
             "mixed_ms_per_call": out["mixed"]["ms_per_call"]}
 
 
+def cutoff_leg(pkg, steps=6, warmup=1, n=4096, seed=1002, tau=0.1, u=6.4):
+    """The distant-pair cutoff configuration: N=4096, Heaviside cutoff c = 0.1
+    (u = 6.4), tau_ext = 0.1.  FP64 dense LU (exact reference order), FP64
+    GMRES and mixed GMRES from the same start over the same accepted steps;
+    device-time dislocation-steps/s and the max position difference against
+    the FP64 dense run."""
+    x, y, _ = pkg.dconf.generate_internal(n, seed)
+    out = {}
+    for name, mode, solver in (("fp64_dense", pkg._lib.D4_PREC_FP64, pkg._lib.D4_SOLVER_DENSE),
+                               ("fp64_gmres", pkg._lib.D4_PREC_FP64, pkg._lib.D4_SOLVER_GMRES),
+                               ("mixed_gmres", pkg._lib.D4_PREC_MIXED, pkg._lib.D4_SOLVER_GMRES)):
+        sd = pkg.SimulationData()
+        sd.set_positions(x, y)
+        sd.precision_mode, sd.solver = mode, solver
+        sd.cutoff_multiplier, sd.heaviside_cutoff = u, True
+        sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
+        eng = pkg.Engine(sd)
+        eng.advance(warmup)
+        r = eng.advance(steps)
+        st = eng.solver_stats()
+        out[name] = dict(value=n * steps / r.device_seconds, attempts=int(r.attempts),
+                         x=eng.positions()[0], stats=st)
+        eng.close()
+    res = {"n": n, "tau_ext": tau, "cutoff_multiplier": u, "heaviside": True, "steps": steps}
+    for name, o in out.items():
+        d, _, _, _ = pkg.dconf.conf_compare(o["x"], y, out["fp64_dense"]["x"], y)
+        res[name] = {"dislocation_steps_per_s": o["value"], "attempts": o["attempts"],
+                     "max_position_diff_vs_fp64_dense": d}
+        if o["stats"]["solves"]:
+            res[name]["gmres_iterations_per_solve"] = (o["stats"]["iterations"] /
+                                                       o["stats"]["solves"])
+            res[name]["gmres_fallbacks"] = o["stats"]["fallbacks"]
+            res[name]["csr_entries"] = o["stats"]["nnz"]
+    res["speedup_mixed_gmres_vs_fp64_dense"] = (out["mixed_gmres"]["value"] /
+                                                out["fp64_dense"]["value"])
+    return res
+
+
+def tabulated_leg(pkg, wl, steps=40):
+    """The N=1024 workload with the tabulated field (1024^2 remainder tables,
+    bicubic) against the analytic field, from the same start."""
+    x, y = start_state(pkg, wl)
+    out = {}
+    for name, field in (("analytic", pkg._lib.D4_FIELD_ANALYTIC),
+                        ("tabulated", pkg._lib.D4_FIELD_TABULATED)):
+        sd = make_sd(pkg, x, y, wl)
+        sd.field = field
+        eng = pkg.Engine(sd)
+        eng.advance(2)
+        r = eng.advance(steps)
+        out[name] = (wl["n"] * steps / r.device_seconds, eng.positions()[0], int(r.attempts))
+        eng.close()
+    d, _, _, _ = pkg.dconf.conf_compare(out["tabulated"][1], y, out["analytic"][1], y)
+    return {"n": wl["n"], "steps": steps, "analytic_dislocation_steps_per_s": out["analytic"][0],
+            "tabulated_dislocation_steps_per_s": out["tabulated"][0],
+            "attempts": [out["analytic"][2], out["tabulated"][2]],
+            "max_position_diff_vs_analytic": d}
+
+
+def ensemble_leg(pkg, count=512, rounds=3, seed=2000):
+    """The ensemble workload: `count` instances, N_k uniform over even values in
+    [64, 2048] (seed 2000), positions seeds 3000 + k, tau_ext = 1e-3 t, time
+    limit 200; one warm-up round (with the initial sweeps), then `rounds`
+    attempt rounds timed on the device."""
+    rng = np.random.default_rng(seed)
+    ns = (rng.integers(32, 1025, size=count) * 2).tolist()
+    cfg = [pkg.dconf.generate_internal(n, 3000 + k)[:2] for k, n in enumerate(ns)]
+    sd = pkg.SimulationData()
+    sd.external_stress = pkg.FixedRateProtocol(0.0, 1e-3)
+    sd.time_limited, sd.time_limit = True, 200.0
+    ens = pkg.Ensemble(sd, cfg)
+    r0 = ens.run(1)
+    r1 = ens.run(rounds)
+    dev = r1[0].device_seconds
+    acc = sum(n * (b.successful_steps - a.successful_steps) for n, a, b in zip(ns, r0, r1))
+    att = sum(n * (b.attempts - a.attempts) for n, a, b in zip(ns, r0, r1))
+    ens.close()
+    return {"instances": count, "sum_n": int(sum(ns)), "n_range": [min(ns), max(ns)],
+            "rounds": rounds, "device_seconds": dev, "s_per_round": dev / rounds,
+            "accepted_dislocation_steps_per_s": acc / dev,
+            "attempted_dislocation_steps_per_s": att / dev}
+
+
+def adjoint_leg(pkg, n=2048, steps=200, seed=1003, tau=0.08, k=20, fd_coords=4):
+    """The adjoint workload: N=2048 (seed 1003), tau_ext = 0.08, 200 accepted
+    steps recorded from the adaptive run; d strain / d (x0, tau0) by the
+    adjoint with checkpoints every 20 steps; checked against the FP64
+    tangent-linear along a random direction and against central differences
+    (h = 1e-6) on `fd_coords` coordinates drawn with seed 4000 (a coordinate
+    whose one-sided quotients disagree by more than 1e-4 is not converged at
+    that h and is reported separately)."""
+    x, y, _ = pkg.dconf.generate_internal(n, seed)
+    sd = pkg.SimulationData()
+    sd.set_positions(x, y)
+    sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
+    e = pkg.Engine(sd)
+    e.record_steps(True)
+    e.advance(steps)
+    t0s, hs = e.recorded_steps()
+    t = time.perf_counter()
+    s0, _ = e.replay(x, t0s, hs)
+    t_rep = time.perf_counter() - t
+    t = time.perf_counter()
+    s, g, gt = e.adjoint(x, t0s, hs, k)
+    t_adj = time.perf_counter() - t
+    rng = np.random.default_rng(4000)
+    d = rng.standard_normal(n)
+    _, ds = e.tangent(x, t0s, hs, d, 0.0)
+    h = 1e-6
+    fd, unconv = [], []
+    for i in rng.choice(n, fd_coords, replace=False):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += h
+        xm[i] -= h
+        sp, sm = e.replay(xp, t0s, hs)[0], e.replay(xm, t0s, hs)[0]
+        q, qp, qm = (sp - sm) / (2 * h), (sp - s0) / h, (s0 - sm) / h
+        rel = abs(q - g[i]) / abs(g[i])
+        (fd if abs(qp - qm) <= 1e-4 * abs(q) else unconv).append(rel)
+    e.close()
+    return {"n": n, "steps": int(len(t0s)), "checkpoint_every": k, "strain": s,
+            "replay_seconds": t_rep, "adjoint_seconds": t_adj,
+            "adjoint_dislocation_steps_per_s": n * len(t0s) / t_adj,
+            "grad_tau0": gt, "tangent_linear_rel_diff": abs(ds - g @ d) / abs(ds),
+            "fd_h": h, "fd_coords": fd_coords, "fd_max_rel_err": max(fd) if fd else None,
+            "fd_unconverged_coords": len(unconv)}
+
+
 def run_reference_arm(args, wl):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -295,6 +428,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the N=4096 mixed vs FP64 leg")
+    ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint",
+                    help="extra single-GPU legs (comma list, or 'none')")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -398,6 +533,16 @@ def main():
             line["mixed_vs_fp64"] = mixed_vs_fp64(pkg)
         except Exception as e:  # pragma: no cover
             line["mixed_vs_fp64"] = {"unavailable": str(e)}
+    legs = [] if args.legs == "none" else args.legs.split(",")
+    for name, fn in (("cutoff", lambda: cutoff_leg(pkg)),
+                     ("tabulated", lambda: tabulated_leg(pkg, wl)),
+                     ("ensemble", lambda: ensemble_leg(pkg)),
+                     ("adjoint", lambda: adjoint_leg(pkg))):
+        if ws == 1 and name in legs:
+            try:
+                line[name] = fn()
+            except Exception as e:  # pragma: no cover
+                line[name] = {"unavailable": str(e)}
     if ws == 1 and not args.no_cpu_baseline:
         try:
             per_step = {64: 0.002, 1024: 0.5, 4096: 25.0}.get(n, 1.0)
