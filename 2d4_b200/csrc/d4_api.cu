@@ -103,7 +103,7 @@ void free_all(Ctx *c) {
     void *bufs[] = {c->x0, c->y, c->xb, c->xh, c->x2, c->xs_tmp, c->ys_tmp, c->v_init,
                     c->v_init2, c->speed, c->speed2, c->dvec, c->dvec_new, c->fac, c->dx,
                     c->tol, c->A, c->LU, c->F, c->piv, c->perm, c->flags, c->red,
-                    c->wave_done, c->wave_done2, c->wave_err, c->xw1, c->xw2,
+                    c->wave_err, c->xw1, c->xw2,
                     c->rowsub, c->rowsc,
                     c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
                     c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
@@ -153,9 +153,8 @@ void sync(Ctx &c) { D4_CUDA_OK(cudaStreamSynchronize(c.stream)); }
 void check_async_errors(Ctx &c) {
     const int *werr = c.h_flags;
     if (werr[0]) {
-        c.err_detail = "triangular solve wavefront timed out: block " + std::to_string(werr[1]) +
-                       " waiting for block " + std::to_string(werr[2]) + " saw flag " +
-                       std::to_string(werr[3]) + ", expected " + std::to_string(werr[4]);
+        c.err_detail = "triangular solve wait timed out: block " + std::to_string(werr[1]) +
+                       " waiting for block " + std::to_string(werr[2]);
         throw d4::StateError(c.err_detail.c_str());
     }
     if (werr[d4::kWaveErrRows]) throw d4::StateError("row-sum pipeline wait timed out");
@@ -427,15 +426,11 @@ int d4_create(void **out, int n, const d4_params *p) {
         dalloc(&c->flags, (size_t)d4::kFlagCount);
         dalloc(&c->red, 8);
         const int nblk = (n + 31) / 32;
-        dalloc(&c->wave_done, (size_t)nblk);
-        dalloc(&c->wave_done2, (size_t)nblk);
         dalloc(&c->wave_err, 8);
         dalloc(&c->xw1, (size_t)n);
         dalloc(&c->xw2, (size_t)n);
         dalloc(&c->rowsub, (size_t)n);
         dalloc(&c->rowsc, (size_t)n);
-        D4_CUDA_OK(cudaMemset(c->wave_done, 0, sizeof(unsigned) * nblk));
-        D4_CUDA_OK(cudaMemset(c->wave_done2, 0, sizeof(unsigned) * nblk));
         D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_red, sizeof(double) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_flags, sizeof(int) * d4::kFlagCount));

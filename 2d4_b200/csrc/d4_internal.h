@@ -25,7 +25,7 @@ enum FlagSlot {
     kFlagCount = 8
 };
 
-// wave_err words: [0..4] wavefront-solve diagnostics, [5] a row-sum pipeline
+// wave_err words: [0..4] triangular-solve wait diagnostics, [5] a row-sum pipeline
 // wait gave up.
 constexpr int kWaveErrRows = 5;
 
@@ -82,10 +82,8 @@ struct Ctx {
     double *h_red = nullptr;
     int *h_flags = nullptr;
 
-    // wavefront triangular solves: per-block done flags (epoch-tagged),
-    // intermediate vectors and the spin-limit error flag
-    unsigned *wave_done = nullptr, *wave_done2 = nullptr;
-    unsigned wave_epoch = 0;
+    // triangular solves: intermediate vectors and the error words of bounded
+    // waits (wave_err, see kWaveErrRows)
     int *wave_err = nullptr;
     double *xw1 = nullptr, *xw2 = nullptr;
     // row sums of the FP64 fused sweep: subSum_i and the row scale (1 + d_i)/2

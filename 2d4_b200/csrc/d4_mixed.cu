@@ -336,30 +336,13 @@ int coop_grid_size32(int n) {
     return g < (n + coop::kThreads - 1) / coop::kThreads ? -1 : g;
 }
 
-// FP32 wavefront solve of LU32 c = r (r FP64 in, c FP32 out).
+// FP32 cluster solve with LU32: c = LU32^-1 r (r FP64 in, c FP32 out).
 static void solve32_once(Ctx &c, const double *r, float *out) {
-    const int nblk = (c.n + 31) / 32;
-    unsigned e1 = ++c.wave_epoch;
-    unsigned e2 = ++c.wave_epoch;
     trsv::GArgs g{};
     g.gmode = -1;
     g.g_in = r;
-    const float *xin_null = nullptr;
-    float *xw1 = c.m_w1, *xw2 = out;
-    void *args1[] = {(void *)&c.n, (void *)&c.LU32, (void *)&c.perm, (void *)&c.flags, (void *)&g,
-                     (void *)&xw1, (void *)&xin_null, (void *)&c.wave_done, (void *)&e1,
-                     (void *)&c.wave_err};
-    const void *fwd = (const void *)trsv::k_trsv_wave<true, float>;
-    const void *bwd = (const void *)trsv::k_trsv_wave<false, float>;
-    D4_CUDA_OK(cudaLaunchCooperativeKernel(fwd, dim3(nblk), dim3(trsv::kWaveThreads), args1, 0,
-                                           c.stream));
-    check_launch("k_trsv_wave<fwd, float>");
-    void *args2[] = {(void *)&c.n, (void *)&c.LU32, (void *)&c.perm, (void *)&c.flags, (void *)&g,
-                     (void *)&xw2, (void *)&xw1, (void *)&c.wave_done2, (void *)&e2,
-                     (void *)&c.wave_err};
-    D4_CUDA_OK(cudaLaunchCooperativeKernel(bwd, dim3(nblk), dim3(trsv::kWaveThreads), args2, 0,
-                                           c.stream));
-    check_launch("k_trsv_wave<bwd, float>");
+    trsv::launch_cluster_solve<float>(c.n, c.LU32, c.perm, c.flags, g, c.m_w1, out, c.wave_err,
+                                      c.stream);
 }
 
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
