@@ -24,7 +24,7 @@ using d4::CudaError;
 namespace d4 {
 std::atomic<long long> g_launches{0};
 
-int prof_begin(Ctx &c, int cat) {
+int prof_begin(Ctx &c, int cat, cudaStream_t st) {
     if (!c.prof.on) return -1;
     if (c.prof.used * 2 + 2 > c.prof.pool.size()) {
         for (int k = 0; k < 64; ++k) {
@@ -36,13 +36,13 @@ int prof_begin(Ctx &c, int cat) {
     const int idx = (int)c.prof.used++;
     if ((size_t)idx >= c.prof.cat.size()) c.prof.cat.resize(idx + 1);
     c.prof.cat[idx] = cat;
-    D4_CUDA_OK(cudaEventRecord(c.prof.pool[2 * idx], c.stream));
+    D4_CUDA_OK(cudaEventRecord(c.prof.pool[2 * idx], st ? st : c.stream));
     return idx;
 }
 
-void prof_end(Ctx &c, int idx) {
+void prof_end(Ctx &c, int idx, cudaStream_t st) {
     if (idx < 0) return;
-    cudaEventRecord(c.prof.pool[2 * idx + 1], c.stream);
+    cudaEventRecord(c.prof.pool[2 * idx + 1], st ? st : c.stream);
 }
 
 void prof_collect(Ctx &c) {
@@ -111,6 +111,15 @@ void free_all(Ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
+    void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
+                  c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
+                  c->xw2_b, c->dx_b};
+    for (void *b : ob)
+        if (b) cudaFree(b);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_copy) cudaEventDestroy(c->ev_copy);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->stream_b) cudaStreamDestroy(c->stream_b);
     if (c->tab) cudaFree(c->tab);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_flags) cudaFreeHost(c->h_flags);
@@ -167,8 +176,151 @@ void read_async_errors(Ctx &c) {
     check_async_errors(c);
 }
 
+// Stages I-IV with stage I on a second stream (FP64 dense form).  Stage I
+// (the big step: LU of A1, two solves, one stress sweep) feeds only the error
+// ratio, and stage II starts from the unfactored A1, so once A1 is copied into
+// stage I's factor buffer the two chains are independent: stage I runs on
+// stream_b with its own factors, force scratch and copies of d and the end
+// speed, while stages II and III run on the context's stream.  The two
+// concurrent cooperative factorisations take half the CTAs each, so both are
+// co-resident; stage III's runs on the full grid.  Every operation is the
+// sequential attempt's, so the results are identical; the factorisations'
+// flags go to separate slots and are read once at the end.
+static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
+    using d4::ProfScope;
+    const d4_protocol &pr = c.p.protocol;
+    const double t1 = t0 + h, th = t0 + h / 2;
+    const int n = c.n;
+    d4::LuBufs L1 = c.lub, L2 = d4::primary_lu(c), L3 = d4::primary_lu(c);
+    L1.flags = c.flags3;
+    L2.flags = c.flags3 + d4::kFlagCount;
+    L3.flags = c.flags3 + 2 * d4::kFlagCount;
+    d4::SolveBufs Sa, Sb;
+    Sa.dvec = c.dvec;
+    Sa.xw1 = c.xw1;
+    Sa.xw2 = c.xw2;
+    Sa.dx = c.dx;
+    Sb.dvec = c.dvec_b;
+    Sb.xw1 = c.xw1_b;
+    Sb.xw2 = c.xw2_b;
+    Sb.dx = c.dx_b;
+    const int half = std::max(1, c.lu_grid / 2);
+    cudaStream_t sa = c.stream, sb = c.stream_b;
+    {
+        ProfScope ps(c, D4_CAT_JACOBIAN);
+        d4::jacobian64(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t1), c.v_init, c.speed);
+    }
+    D4_CUDA_OK(cudaMemcpyAsync(c.dvec_b, c.dvec, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
+    D4_CUDA_OK(cudaMemcpyAsync(c.speed_b, c.speed, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
+    D4_CUDA_OK(cudaEventRecord(c.ev_fork, sa));
+    D4_CUDA_OK(cudaStreamWaitEvent(sb, c.ev_fork, 0));
+    // stage I on stream_b
+    {
+        ProfScope ps(c, D4_CAT_FACTOR, sb);
+        d4::factor64_async(c, L1, c.A, half, sb, c.ev_copy);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE, sb);
+        d4::solve_update64_with(c, L1, Sb, sb, d4::kGBig, h, c.speed_b, c.v_init, nullptr, nullptr,
+                                c.x0, c.xb);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS, sb);
+        d4::speeds64_with(c, c.F_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE, sb);
+        d4::solve_update64_with(c, L1, Sb, sb, d4::kGNewton, h, c.speed2_b, c.v_init, c.xb, c.x0,
+                                c.xb, c.xb);
+    }
+    D4_CUDA_OK(cudaEventRecord(c.ev_join, sb));
+    // stage II on the context's stream, once A1 is copied
+    D4_CUDA_OK(cudaStreamWaitEvent(sa, c.ev_copy, 0));
+    {
+        ProfScope ps(c, D4_CAT_RESCALE);
+        d4::jacobian_from_prev64(c, (th - t0) / (t1 - t0));
+    }
+    {
+        ProfScope ps(c, D4_CAT_FACTOR);
+        d4::factor64_async(c, L2, c.A, half, sa, nullptr);
+    }
+    d4::shift_speed64(c, c.speed, ext_stress(pr, th) - ext_stress(pr, t1));
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update64_with(c, L2, Sa, sa, d4::kGHalf, h, c.speed, c.v_init, nullptr, nullptr,
+                                c.x0, c.xh);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS);
+        d4::speeds64(c, c.xh, c.y, ext_stress(pr, th), c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update64_with(c, L2, Sa, sa, d4::kGNewton, h / 2, c.speed2, c.v_init, c.xh, c.x0,
+                                c.xh, c.xh);
+    }
+    // stage III
+    {
+        ProfScope ps(c, D4_CAT_JACOBIAN);
+        d4::jacobian64(c, c.xh, c.y, h / 2, ext_stress(pr, th), ext_stress(pr, t1), c.v_init2,
+                       c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_FACTOR);
+        d4::factor64_async(c, L3, c.A, c.lu_grid, sa, nullptr);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update64_with(c, L3, Sa, sa, d4::kGHalf, h, c.speed2, c.v_init2, nullptr, nullptr,
+                                c.xh, c.x2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS);
+        d4::speeds64(c, c.x2, c.y, ext_stress(pr, t1), c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update64_with(c, L3, Sa, sa, d4::kGNewton, h / 2, c.speed2, c.v_init2, c.x2,
+                                c.xh, c.x2, c.x2);
+    }
+    D4_CUDA_OK(cudaStreamWaitEvent(sa, c.ev_join, 0));
+    d4::error_ratio64(c, c.xb, c.x2);
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, sa));
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.wave_err, sizeof(int) * 6, cudaMemcpyDeviceToHost, sa));
+    int fl[3 * d4::kFlagCount];
+    D4_CUDA_OK(cudaMemcpyAsync(fl, c.flags3, sizeof(fl), cudaMemcpyDeviceToHost, sa));
+    sync(c);
+    if (c.prof.on) d4::prof_collect(c);
+    check_async_errors(c);
+    int singular = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (fl[k * d4::kFlagCount + d4::kFlagBarrierTimeout])
+            throw d4::StateError("LU grid barrier timed out");
+        singular |= fl[k * d4::kFlagCount + d4::kFlagSingular] != 0;
+    }
+    // the last factorisation's flags stand for the context's (d4_solve etc.)
+    D4_CUDA_OK(cudaMemcpyAsync(c.flags, L3.flags, sizeof(int) * d4::kFlagCount,
+                               cudaMemcpyDeviceToDevice, sa));
+    c.factor_singular = fl[2 * d4::kFlagCount + d4::kFlagSingular] != 0;
+    c.factor_pivoted = 0;
+    *singular_out = singular;
+}
+
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
+    if (c.overlap) {
+        int singular = 0;
+        attempt_overlap(c, t0, h, &singular);
+        const int idx = (int)c.h_red[1];
+        if (idx >= 0) c.selected_id = idx;
+        res->ratio = c.h_red[0] / c.dipole_prec_sq;
+        res->max_id = c.selected_id;
+        res->accepted = res->ratio < 1;
+        res->singular = singular;
+        res->pivoted = 0;
+        res->refine_residual = 0;
+        return D4_OK;
+    }
     using d4::ProfScope;
     const d4_protocol &pr = c.p.protocol;
     const double t_1__ = t0 + h;
@@ -453,6 +605,26 @@ int d4_create(void **out, int n, const d4_params *p) {
         }
         c->use_gmres = d4::gmres_selected(*c) ? 1 : 0;
         if (c->use_gmres) d4::sparse_alloc(*c);
+        if (!mixed && !c->use_gmres) {
+            // stage I's own stream and buffers (attempt_overlap)
+            c->overlap = 1;
+            D4_CUDA_OK(cudaStreamCreateWithFlags(&c->stream_b, cudaStreamNonBlocking));
+            D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming));
+            D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+            dalloc(&c->lub.LU, nn);
+            dalloc(&c->lub.P0, (size_t)n * 32);
+            dalloc(&c->lub.Q, (size_t)n * 64);
+            dalloc(&c->lub.mask, (size_t)c->lu_mask_words);
+            dalloc(&c->lub.bar, 64);
+            dalloc(&c->lub.perm, (size_t)n);
+            dalloc(&c->lub.piv, (size_t)n);
+            dalloc(&c->flags3, (size_t)3 * d4::kFlagCount);
+            dalloc(&c->F_b, nn);
+            double **bv[] = {&c->dvec_b, &c->speed_b, &c->speed2_b, &c->xw1_b, &c->xw2_b,
+                             &c->dx_b};
+            for (double **v : bv) dalloc(v, (size_t)n);
+        }
         d4::reset_tol64(*c);
         sync(*c);
     } catch (const CudaError &e) {

@@ -133,11 +133,11 @@ static PairArgs pair_args(Ctx &c, const double *x, const double *y) {
 }
 
 template <bool kJac>
-static void launch_rows(Ctx &c, const RowArgs &r) {
+static void launch_rows(Ctx &c, const RowArgs &r, cudaStream_t st) {
     constexpr int bytes = row_smem_bytes<kJac>();
     D4_CUDA_OK(cudaFuncSetAttribute(k_rows64<kJac>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     bytes));
-    k_rows64<kJac><<<(c.n + kRowRows - 1) / kRowRows, 64, bytes, c.stream>>>(r);
+    k_rows64<kJac><<<(c.n + kRowRows - 1) / kRowRows, 64, bytes, st>>>(r);
     check_launch(kJac ? "k_rows64<jacobian>" : "k_rows64<speeds>");
 }
 
@@ -146,20 +146,26 @@ static int pair_blocks(int n) {
     return T * (T + 1) / 2;
 }
 
-void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v) {
+void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
+                   double ext, double *v) {
     PairArgs a = pair_args(c, x, y);
+    a.F = F;
     if (c.tab)
-        k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+        k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, st>>>(a);
     else
-        k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+        k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, st>>>(a);
     check_launch("k_pairs64<speeds>");
     RowArgs r{};
     r.n = c.n;
-    r.F = c.F;
+    r.F = F;
     r.ext_a = ext;
     r.v_a = v;
     r.err = c.wave_err + kWaveErrRows;
-    launch_rows<false>(c, r);
+    launch_rows<false>(c, r, st);
+}
+
+void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v) {
+    speeds64_with(c, c.F, c.stream, x, y, ext, v);
 }
 
 void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
@@ -184,7 +190,7 @@ void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a
     r.rowsc = c.rowsc;
     r.wfn = c.p.weight_function;
     r.err = c.wave_err + kWaveErrRows;
-    launch_rows<true>(c, r);
+    launch_rows<true>(c, r, c.stream);
     k_scale_rows64<<<blocks((long long)c.n * c.n, 256), 256, 0, c.stream>>>(c.n, c.A, c.rowsub,
                                                                            c.rowsc);
     check_launch("k_scale_rows64");

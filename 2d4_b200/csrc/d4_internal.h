@@ -29,6 +29,20 @@ enum FlagSlot {
 // wait gave up.
 constexpr int kWaveErrRows = 5;
 
+// Buffers of one LU factorisation (factors, pivot bookkeeping, flags).
+struct LuBufs {
+    double *LU = nullptr, *P0 = nullptr, *Q = nullptr;
+    unsigned *mask = nullptr, *bar = nullptr;
+    int *flags = nullptr, *perm = nullptr, *piv = nullptr;
+};
+
+// Buffers of the solves of one stage chain: the weights read by the
+// residual, the forward-solve scratch and the correction.
+struct SolveBufs {
+    const double *dvec = nullptr;
+    double *xw1 = nullptr, *xw2 = nullptr, *dx = nullptr;
+};
+
 // State of Simulation::run's loop kept between d4_advance calls.
 struct RunState {
     bool started = false;
@@ -122,20 +136,34 @@ struct Ctx {
     bool recording = false;
     std::vector<double> rec_t0, rec_h;
 
+    // stage I (the big step) on a second stream, concurrent with stages II
+    // and III (FP64 dense form): its own factorisation, force scratch,
+    // weights and speed copies, solve scratch, and the three factorisations'
+    // flags of an attempt
+    int overlap = 0;
+    cudaStream_t stream_b = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_copy = nullptr, ev_join = nullptr;
+    LuBufs lub;
+    double *F_b = nullptr, *dvec_b = nullptr, *speed_b = nullptr, *speed2_b = nullptr,
+           *xw1_b = nullptr, *xw2_b = nullptr, *dx_b = nullptr;
+    int *flags3 = nullptr;  // 3 x kFlagCount
+
     RunState rs;
     Prof prof;
 };
 
 // Category timing: returns the index of an event pair (or -1 when off).
-int prof_begin(Ctx &c, int cat);
-void prof_end(Ctx &c, int idx);
+int prof_begin(Ctx &c, int cat, cudaStream_t st = nullptr);  // null: the context's stream
+void prof_end(Ctx &c, int idx, cudaStream_t st = nullptr);
 void prof_collect(Ctx &c);  // after a stream sync: folds finished pairs into totals
 
 struct ProfScope {
     Ctx &c;
     int idx;
-    ProfScope(Ctx &cc, int cat) : c(cc), idx(prof_begin(cc, cat)) {}
-    ~ProfScope() { prof_end(c, idx); }
+    cudaStream_t st;
+    ProfScope(Ctx &cc, int cat, cudaStream_t s = nullptr)
+        : c(cc), idx(prof_begin(cc, cat, s)), st(s) {}
+    ~ProfScope() { prof_end(c, idx, st); }
 };
 
 extern std::atomic<long long> g_launches;
@@ -160,11 +188,20 @@ void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double 
 // Factorises A into LU; returns via flags whether the pivoted path ran and
 // whether the matrix is singular.  Host-synchronising.
 int factor64(Ctx &c);                 // d4_lu_coop64.cu
+void factor64_async(Ctx &c, const LuBufs &L, const double *A, int grid, cudaStream_t st,
+                    cudaEvent_t after_copy);
+LuBufs primary_lu(Ctx &c);
 int coop_grid_size(int n);            // CTAs of the cooperative LU (-1: n too large)
 enum GMode { kGBig = 0, kGHalf = 1, kGNewton = 2 };
 // g built from (gmode, hval, dvec, s_end, s_init, x_new, x_old); solve; out = base - dx.
 void solve_update64(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
+void solve_update64_with(Ctx &c, const LuBufs &L, const SolveBufs &S, cudaStream_t st, int gmode,
+                         double hval, const double *s_end, const double *s_init,
+                         const double *x_new, const double *x_old, const double *base,
+                         double *out);
+void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
+                   double ext, double *v);
 // Plain solve of A dx = g (g on device, dx written to c.dx).
 void solve_plain64(Ctx &c, const double *g);
 

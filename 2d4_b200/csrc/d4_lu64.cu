@@ -37,6 +37,26 @@ void solve_update64(Ctx &c, int gmode, double hval, const double *s_end, const d
     launch_solve(c, ga);
 }
 
+void solve_update64_with(Ctx &c, const LuBufs &L, const SolveBufs &S, cudaStream_t st, int gmode,
+                         double hval, const double *s_end, const double *s_init,
+                         const double *x_new, const double *x_old, const double *base,
+                         double *out) {
+    GArgs ga{};
+    ga.gmode = gmode;
+    ga.hval = hval;
+    ga.dvec = S.dvec;
+    ga.s_end = s_end;
+    ga.s_init = s_init;
+    ga.x_new = x_new;
+    ga.x_old = x_old;
+    ga.base = base;
+    ga.out = out;
+    ga.dx_out = S.dx;
+    ga.fix_singular = 1;
+    trsv::launch_cluster_solve<double>(c.n, L.LU, L.perm, L.flags, ga, S.xw1, S.xw2, c.wave_err,
+                                       st);
+}
+
 void solve_plain64(Ctx &c, const double *g) {
     GArgs ga{};
     ga.gmode = -1;

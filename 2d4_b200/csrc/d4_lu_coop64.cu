@@ -52,28 +52,50 @@ int coop_grid_size(int n) {
     return g;
 }
 
-int factor64(Ctx &c) {
+// Factorises A into L.LU on `st` with `grid` CTAs, without waiting: flags
+// (L.flags) are read by the caller later.  `after_copy` (may be null) is
+// recorded once A has been copied, after which A may change.
+void factor64_async(Ctx &c, const LuBufs &L, const double *A, int grid, cudaStream_t st,
+                    cudaEvent_t after_copy) {
     const int n = c.n;
     const size_t bytes = sizeof(double) * (size_t)n * n;
-    D4_CUDA_OK(cudaMemsetAsync(c.flags, 0, sizeof(int) * kFlagCount, c.stream));
-    D4_CUDA_OK(cudaMemsetAsync(c.lu_bar, 0, sizeof(unsigned) * 64, c.stream));
-    D4_CUDA_OK(cudaMemsetAsync(c.lu_mask, 0, sizeof(unsigned) * c.lu_mask_words, c.stream));
-    D4_CUDA_OK(cudaMemcpyAsync(c.LU, c.A, bytes, cudaMemcpyDeviceToDevice, c.stream));
+    D4_CUDA_OK(cudaMemsetAsync(L.flags, 0, sizeof(int) * kFlagCount, st));
+    D4_CUDA_OK(cudaMemsetAsync(L.bar, 0, sizeof(unsigned) * 64, st));
+    D4_CUDA_OK(cudaMemsetAsync(L.mask, 0, sizeof(unsigned) * c.lu_mask_words, st));
+    D4_CUDA_OK(cudaMemcpyAsync(L.LU, A, bytes, cudaMemcpyDeviceToDevice, st));
+    if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
     coop::CoopArgs<double> a;
     a.n = n;
-    a.A = c.LU;
-    a.P0 = c.lu_p0;
-    a.Q = c.lu_q;
-    a.mask = c.lu_mask;
-    a.piv = c.piv;
-    a.flags = c.flags;
-    a.bar = c.lu_bar;
-    a.perm = c.perm;
+    a.A = L.LU;
+    a.P0 = L.P0;
+    a.Q = L.Q;
+    a.mask = L.mask;
+    a.piv = L.piv;
+    a.flags = L.flags;
+    a.bar = L.bar;
+    a.perm = L.perm;
     void *args[] = {(void *)&a};
-    D4_CUDA_OK(cudaLaunchCooperativeKernel((const void *)coop::k_lu_coop<double>, dim3(c.lu_grid),
+    D4_CUDA_OK(cudaLaunchCooperativeKernel((const void *)coop::k_lu_coop<double>, dim3(grid),
                                            dim3(coop::kThreads), args,
-                                           coop::kRowBufBytes<double>(), c.stream));
+                                           coop::kRowBufBytes<double>(), st));
     check_launch("k_lu_coop<double>");
+}
+
+LuBufs primary_lu(Ctx &c) {
+    LuBufs L;
+    L.LU = c.LU;
+    L.P0 = c.lu_p0;
+    L.Q = c.lu_q;
+    L.mask = c.lu_mask;
+    L.bar = c.lu_bar;
+    L.flags = c.flags;
+    L.perm = c.perm;
+    L.piv = c.piv;
+    return L;
+}
+
+int factor64(Ctx &c) {
+    factor64_async(c, primary_lu(c), c.A, c.lu_grid, c.stream, nullptr);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
                                cudaMemcpyDeviceToHost, c.stream));
     D4_CUDA_OK(cudaStreamSynchronize(c.stream));
