@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(kLuT) k_ens_lu(Pools P, const Inst *ins, const
     __shared__ double rv[kLuT / 32];
     __shared__ int ri[kLuT / 32];
     __shared__ int s_piv;
+    __shared__ double prow[kPan];
     const int k = act[blockIdx.x];
     const Inst in = ins[k];
     const int n = in.n, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(kLuT) k_ens_lu(Pools P, const Inst *ins, const
             const double akk = fabs(a[kk + (size_t)kk * n]);
             double bv = -1;
             int bi = -1;
+#pragma unroll 4
             for (int i = kk + 1 + tid; i < n; i += kLuT) {
                 const double v = fabs(a[i + (size_t)kk * n]);
                 if (v > bv) {
@@ -271,13 +273,25 @@ __global__ void __launch_bounds__(kLuT) k_ens_lu(Pools P, const Inst *ins, const
                 }
             __syncthreads();
             const double d = a[kk + (size_t)kk * n];
+#pragma unroll 4
             for (int i = kk + 1 + tid; i < n; i += kLuT) a[i + (size_t)kk * n] /= d;
             __syncthreads();
-            const int rows = n - kk - 1, cols = k0 + kw - kk - 1;
-            for (int idx = tid; idx < rows * cols; idx += kLuT) {
-                const int i = kk + 1 + idx % rows, j = kk + 1 + idx / rows;
-                const double t = a[kk + (size_t)j * n];
-                if (t != 0.0) a[i + (size_t)j * n] -= a[i + (size_t)kk * n] * t;
+            // rank-1 update of the panel's remaining columns: a thread per row,
+            // the row's loads issued together (one memory round trip per row)
+            const int ncol = k0 + kw - kk - 1;
+            if (tid < kPan) prow[tid] = tid < ncol ? a[kk + (size_t)(kk + 1 + tid) * n] : 0.0;
+            __syncthreads();
+            for (int i = kk + 1 + tid; i < n; i += kLuT) {
+                const double l = a[i + (size_t)kk * n];
+                double v[kPan - 1];
+#pragma unroll
+                for (int q = 0; q < kPan - 1; ++q)
+                    v[q] = q < ncol ? a[i + (size_t)(kk + 1 + q) * n] : 0.0;
+#pragma unroll
+                for (int q = 0; q < kPan - 1; ++q) {
+                    const double t = prow[q];
+                    if (q < ncol && t != 0.0) a[i + (size_t)(kk + 1 + q) * n] = v[q] - l * t;
+                }
             }
             __syncthreads();
         }
