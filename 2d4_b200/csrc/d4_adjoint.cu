@@ -20,7 +20,7 @@
 // every K steps, then for each segment recomputes its steps storing the stage
 // quantities and the transposed LU factors, and sweeps back with transposed
 // solves A^T mu = lambda through those factors (P A = L U:
-// A^T = U^T L^T P).
+// A^T = U^T L^T P), run by the cluster solve of d4_trsv.cuh.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -29,11 +29,14 @@
 
 #include "d4_field_dual.cuh"
 #include "d4_internal.h"
+#include "d4_trsv.cuh"
 
 namespace d4 {
 namespace adj {
 
 __device__ __forceinline__ double bsg(int i, int n) { return i < n / 2 ? 1.0 : -1.0; }
+
+inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
 
 // ---- pair reductions with the field's first and second x-derivatives ----
 //
@@ -64,8 +67,12 @@ struct DerivArgs {
 //           o3 = sum bb tt (a_i - a_j)(r_i - r_j), o4 = Jt q, o5 = Jt r
 // kModeVjp: o0 = sum bb [sp (a_i - a_j) + tt ((p_i - p_j)(q_i - q_j)
 //                         + (r_i - r_j)(s_i - s_j) + (u_i + u_j))]
+// Grid: (row tiles, column tiles) of kPT x kPT pairs; block (bx, by) sums the
+// pairs of its rows with the columns of tile by and writes the partial sums to
+// part[(out * tiles + by) * n + i]; k_deriv_sum then adds the tiles in order
+// (deterministic results).
 template <int kMode>
-__global__ void __launch_bounds__(kPT) k_deriv(DerivArgs A) {
+__global__ void __launch_bounds__(kPT) k_deriv(DerivArgs A, double *part) {
     __shared__ double sx[kPT], sy[kPT], s1[kPT], s2[kPT], s3[kPT], s4[kPT], s5[kPT], s6[kPT];
     const int n = A.n;
     const int i = blockIdx.x * kPT + threadIdx.x;
@@ -88,9 +95,9 @@ __global__ void __launch_bounds__(kPT) k_deriv(DerivArgs A) {
         }
     }
     double o[6] = {0, 0, 0, 0, 0, 0};
-    for (int j0 = 0; j0 < n; j0 += kPT) {
+    {
+        const int j0 = blockIdx.y * kPT;
         const int j = j0 + threadIdx.x;
-        __syncthreads();
         if (j < n) {
             sx[threadIdx.x] = A.x[j];
             sy[threadIdx.x] = A.y[j];
@@ -109,8 +116,7 @@ __global__ void __launch_bounds__(kPT) k_deriv(DerivArgs A) {
             }
         }
         __syncthreads();
-        if (!own) continue;
-        const int jn = min(kPT, n - j0);
+        const int jn = own ? min(kPT, n - j0) : 0;
         for (int t = 0; t < jn; ++t) {
             const int jj = j0 + t;
             if (jj == i) continue;
@@ -155,70 +161,41 @@ __global__ void __launch_bounds__(kPT) k_deriv(DerivArgs A) {
     const int nout = (kMode == kModeJv || kMode == kModeJt) ? (A.o[1] ? 2 : 1)
                      : kMode == kModeJvp                   ? 6
                                                            : 1;
-    for (int k = 0; k < nout; ++k) A.o[k][i] = o[k];
+    for (int k = 0; k < nout; ++k) part[((size_t)k * gridDim.y + blockIdx.y) * n + i] = o[k];
 }
 
-// ---- transposed solve with LU factors stored transposed (one CTA) ----
-constexpr int kTT = 512;
+__global__ void k_deriv_sum(int n, int tiles, int nout, const double *part, DerivArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = 0; k < nout; ++k) {
+        double v = 0;
+        for (int t = 0; t < tiles; ++t) v += part[((size_t)k * tiles + t) * n + i];
+        A.o[k][i] = v;
+    }
+}
 
-// Solves A^T mu = lam with Lt = (LU)^T column-major (P A = L U, perm[r] = the
-// original row of position r): U^T z = lam (forward, lower, divided), then
-// L^T w = z (backward, unit upper), then mu[perm[r]] = w[r].  32-row blocks:
-// warp 0 resolves the block's triangle with shuffles, then every thread applies
-// the block's 32 values to its rows (coalesced columns of Lt).
-__global__ void __launch_bounds__(kTT) k_trsv_t(int n, const double *__restrict__ Lt,
-                                                const int *__restrict__ perm, const double *lam,
-                                                double *mu) {
-    extern __shared__ double xs[];
-    __shared__ double blk[32];
-    const int tid = threadIdx.x, lane = tid & 31;
-    for (int i = tid; i < n; i += kTT) xs[i] = lam[i];
-    __syncthreads();
-    for (int kb = 0; kb < n; kb += 32) {
-        const int kw = min(32, n - kb);
-        if (tid < 32) {
-            double x = lane < kw ? xs[kb + lane] : 0;
-            for (int k = 0; k < kw; ++k) {
-                if (lane == k) x = x / Lt[(size_t)(kb + k) + (size_t)(kb + k) * n];
-                const double t = __shfl_sync(0xffffffffu, x, k);
-                if (lane > k && lane < kw) x -= Lt[(size_t)(kb + lane) + (size_t)(kb + k) * n] * t;
-            }
-            if (lane < kw) {
-                xs[kb + lane] = x;
-                blk[lane] = x;
-            }
-        }
-        __syncthreads();
-        for (int i = kb + kw + tid; i < n; i += kTT) {
-            double acc = xs[i];
-            for (int k = 0; k < kw; ++k) acc -= Lt[(size_t)i + (size_t)(kb + k) * n] * blk[k];
-            xs[i] = acc;
-        }
-        __syncthreads();
-    }
-    const int nb = (n + 31) / 32;
-    for (int b = nb - 1; b >= 0; --b) {
-        const int kb = b * 32, kw = min(32, n - kb);
-        if (tid < 32) {
-            double x = lane < kw ? xs[kb + lane] : 0;
-            for (int k = kw - 1; k >= 0; --k) {
-                const double t = __shfl_sync(0xffffffffu, x, k);
-                if (lane < k) x -= Lt[(size_t)(kb + lane) + (size_t)(kb + k) * n] * t;
-            }
-            if (lane < kw) {
-                xs[kb + lane] = x;
-                blk[lane] = x;
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < kb; i += kTT) {
-            double acc = xs[i];
-            for (int k = 0; k < kw; ++k) acc -= Lt[(size_t)i + (size_t)(kb + k) * n] * blk[k];
-            xs[i] = acc;
-        }
-        __syncthreads();
-    }
-    for (int r = tid; r < n; r += kTT) mu[perm[r]] = xs[r];
+// Launches k_deriv<kMode> over all pair tiles and the in-order tile sum.
+template <int kMode>
+void run_deriv(Ctx &c, DerivArgs &A, double *part) {
+    const int tiles = nb(c.n, kPT);
+    const int nout = (kMode == kModeJv || kMode == kModeJt) ? (A.o[1] ? 2 : 1)
+                     : kMode == kModeJvp                   ? 6
+                                                           : 1;
+    k_deriv<kMode><<<dim3(tiles, tiles), kPT, 0, c.stream>>>(A, part);
+    check_launch("k_deriv");
+    k_deriv_sum<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, tiles, nout, part, A);
+    check_launch("k_deriv_sum");
+}
+
+// Transposed solve A^T mu = lam with the factors stored transposed (Lt) and
+// perm (P A = L U), by the cluster solve in its transposed mode.
+void trsv_t(Ctx &c, const double *Lt, const int *perm, const double *lam, double *mu,
+            double *scratch) {
+    trsv::GArgs g{};
+    g.gmode = -1;
+    g.g_in = lam;
+    trsv::launch_cluster_solve<double, true>(c.n, Lt, perm, c.flags, g, scratch, mu, c.wave_err,
+                                             c.stream);
 }
 
 __global__ void k_transpose(int n, const double *__restrict__ a, double *__restrict__ t) {
@@ -366,8 +343,6 @@ __global__ void __launch_bounds__(1024) k_bdot(int n, const double *x, const dou
     }
 }
 
-inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
-
 // Device pointers of one stage, valid during the stage hook.
 struct Stage {
     const double *z, *x1, *d1, *d2, *d, *va, *vb, *v1b;
@@ -479,8 +454,8 @@ struct Replay {
 
 // o0 = J a, o1 = J cc (cc may be null) for J = Jv (velocities) or Jt (matrix).
 template <int kMode>
-void deriv_j(Ctx &c, const double *x, const double *a, const double *cc, double *o0,
-             double *o1) {
+void deriv_j(Ctx &c, double *part, const double *x, const double *a, const double *cc,
+             double *o0, double *o1) {
     DerivArgs A{};
     A.n = c.n;
     A.x = x;
@@ -489,8 +464,7 @@ void deriv_j(Ctx &c, const double *x, const double *a, const double *cc, double 
     A.c = cc;
     A.o[0] = o0;
     A.o[1] = o1;
-    k_deriv<kMode><<<nb(c.n, kPT), kPT, 0, c.stream>>>(A);
-    check_launch(kMode == kModeJv ? "k_deriv<jv>" : "k_deriv<jt>");
+    run_deriv<kMode>(c, A, part);
 }
 
 // Validates the context for differentiation: FP64 analytic field with every
@@ -592,6 +566,7 @@ int d4_tangent(void *ctx, long long steps, const double *t0s, const double *hs,
                                    c->stream));
         double *dz = w.alloc(n), *dzs = w.alloc(n), *dx1 = w.alloc(n), *dd = w.alloc(n),
                *rhs = w.alloc(n), *jx1 = w.alloc(n);
+        double *part = w.alloc((size_t)6 * nb(n, kPT) * n);
         double *o[6];
         for (double *&p : o) p = w.alloc(n);
         D4_CUDA_OK(cudaMemcpyAsync(dz, dx0, sizeof(double) * n, cudaMemcpyHostToDevice,
@@ -609,15 +584,14 @@ int d4_tangent(void *ctx, long long steps, const double *t0s, const double *hs,
             A.q = s.d1;
             A.r = s.d2;
             for (int k = 0; k < 6; ++k) A.o[k] = o[k];
-            k_deriv<kModeJvp><<<nb(n, kPT), kPT, 0, c->stream>>>(A);
-            d4::check_launch("k_deriv<jvp>");
+            run_deriv<kModeJvp>(*c, A, part);
             k_tl_rhs1<<<nb(n, 256), 256, 0, c->stream>>>(n, s.k, dtau0, s.d, s.va, s.vb, o[0],
                                                           o[1], o[2], o[4], dd, rhs);
             d4::check_launch("k_tl_rhs1");
             d4::solve_plain64(*c, rhs);
             k_sub<<<nb(n, 256), 256, 0, c->stream>>>(n, dz, c->dx, dx1);
             d4::check_launch("k_sub");
-            deriv_j<kModeJv>(*c, s.x1, dx1, nullptr, jx1, nullptr);
+            deriv_j<kModeJv>(*c, part, s.x1, dx1, nullptr, jx1, nullptr);
             k_tl_rhs2<<<nb(n, 256), 256, 0, c->stream>>>(n, s.k, dtau0, s.d, s.va, s.v1b, dz,
                                                           dx1, jx1, o[0], o[3], o[5], dd, rhs);
             d4::check_launch("k_tl_rhs2");
@@ -680,10 +654,9 @@ int d4_adjoint(void *ctx, long long steps, const double *t0s, const double *hs,
                *dmu = w.alloc(n), *w1 = w.alloc(n), *lx1 = w.alloc(n), *jd1 = w.alloc(n),
                *jd2 = w.alloc(n), *ea = w.alloc(n), *eq = w.alloc(n), *es = w.alloc(n),
                *eu = w.alloc(n), *oz = w.alloc(n);
+        double *part = w.alloc((size_t)6 * nb(n, kPT) * n);
         D4_CUDA_OK(cudaMemsetAsync(lam_next, 0, sizeof(double) * n, c->stream));
-        const int trsv_smem = (int)(sizeof(double) * n);
-        D4_CUDA_OK(cudaFuncSetAttribute(k_trsv_t, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        trsv_smem));
+        double *tsc = w.alloc(n);  // forward-pass result of the transposed solves
         for (long long seg = nseg - 1; seg >= 0; --seg) {
             const long long k0 = seg * K, k1 = std::min<long long>(steps, k0 + K);
             D4_CUDA_OK(cudaMemcpyAsync(c->x0, ckpt + (size_t)seg * n, sizeof(double) * n,
@@ -717,18 +690,16 @@ int d4_adjoint(void *ctx, long long steps, const double *t0s, const double *hs,
                     const int *pm = tperm + slot * n;
                     const StageCoef &kc = tk[slot];
                     // mu2 = A^-T lam; lam_x1 = lam - mu2 + hh Jv(x1) (D mu2)
-                    k_trsv_t<<<1, kTT, trsv_smem, c->stream>>>(n, Lt, pm, lam, mu2);
-                    d4::check_launch("k_trsv_t");
+                    trsv_t(*c, Lt, pm, lam, mu2, tsc);
                     k_scale_d<<<nb(n, 256), 256, 0, c->stream>>>(n, Dv, mu2, dmu);
                     d4::check_launch("k_scale_d");
-                    deriv_j<kModeJv>(*c, X1, dmu, nullptr, w1, nullptr);
+                    deriv_j<kModeJv>(*c, part, X1, dmu, nullptr, w1, nullptr);
                     k_adj_x1<<<nb(n, 256), 256, 0, c->stream>>>(n, kc, lam, mu2, w1, lx1);
                     d4::check_launch("k_adj_x1");
                     // mu1 = A^-T lam_x1
-                    k_trsv_t<<<1, kTT, trsv_smem, c->stream>>>(n, Lt, pm, lx1, mu1);
-                    d4::check_launch("k_trsv_t");
+                    trsv_t(*c, Lt, pm, lx1, mu1, tsc);
                     // z sweep
-                    deriv_j<kModeJt>(*c, Z, D1, D2, jd1, jd2);
+                    deriv_j<kModeJt>(*c, part, Z, D1, D2, jd1, jd2);
                     k_adj_z<<<1, 1024, 0, c->stream>>>(n, kc, Dv, mu1, mu2, VA, VB, V1B, jd1,
                                                        jd2, ea, eq, es, eu, sd + 1);
                     d4::check_launch("k_adj_z");
@@ -743,8 +714,7 @@ int d4_adjoint(void *ctx, long long steps, const double *t0s, const double *hs,
                     A.s = es;
                     A.u = eu;
                     A.o[0] = oz;
-                    k_deriv<kModeVjp><<<nb(n, kPT), kPT, 0, c->stream>>>(A);
-                    d4::check_launch("k_deriv<vjp>");
+                    run_deriv<kModeVjp>(*c, A, part);
                     k_adj_out<<<nb(n, 256), 256, 0, c->stream>>>(n, mu2, lx1, oz, lam);
                     d4::check_launch("k_adj_out");
                 }

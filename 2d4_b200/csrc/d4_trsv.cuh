@@ -142,7 +142,11 @@ __device__ __forceinline__ void tile_regs(const T *__restrict__ LU, int n, int b
     }
 }
 
-template <bool kFwd, typename T>
+// kTrans: the factors are given transposed (Lt = (LU)^T) and the system is
+// A^T x = g (P A = L U, so A^T = U^T L^T P): the forward pass is U^T (lower,
+// divided), the backward pass L^T (unit upper), g is taken unpermuted and the
+// result scattered through perm at the end.
+template <bool kFwd, typename T, bool kTrans = false>
 __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
     int n, const T *__restrict__ LU, const int *__restrict__ perm, const int *__restrict__ flags,
     GArgs ga, T *xg, const T *xin, int *err) {
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
         const int b = kFwd ? first + m * stride : first + (nmine - 1 - m) * stride;
         const int row = b * 32 + lane;
         const bool row_ok = row < n;
-        T xi = row_ok ? (kFwd ? T(g_of(ga, perm[row])) : xin[row]) : T(0);
+        T xi = row_ok ? (kFwd ? T(kTrans ? ga.g_in[row] : g_of(ga, perm[row])) : xin[row]) : T(0);
         T tl[32];
         // the diagonal tile, early, into this warp's shared slot (row per lane)
         tile_regs(LU, n, b, b, lane, tl);
@@ -225,13 +229,14 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
         if (kFwd) {
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
+                if (kTrans && k < kw && lane == k) xi = xi / dt[k][k];
                 const T t = __shfl_sync(0xffffffffu, xi, k);
                 if (k < kw && lane > k && t != T(0)) xi = xi - dt[lane][k] * t;
             }
         } else {
 #pragma unroll
             for (int k = 31; k >= 0; --k) {
-                if (k < kw && lane == k) xi = xi / dt[k][k];
+                if (!kTrans && k < kw && lane == k) xi = xi / dt[k][k];
                 const T t = __shfl_sync(0xffffffffu, xi, k);
                 if (k < kw && lane < k && t != T(0)) xi = xi - dt[lane][k] * t;
             }
@@ -242,8 +247,8 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
         if (row_ok)
             for (int q = 0; q < C; ++q) st_async(mapa(xa, (unsigned)q), xi, mapa(mba, (unsigned)q));
         if (row_ok) {
-            xg[row] = xi;
-            if (!kFwd) {
+            xg[(kTrans && !kFwd) ? perm[row] : row] = xi;
+            if (!kFwd && !kTrans) {
                 double d = (double)xi;
                 if (ga.fix_singular && flags[kFlagSingular] && !((-1 < d) && (d < 1))) d = 0;
                 if (ga.dx_out) ga.dx_out[row] = d;
@@ -257,7 +262,7 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
 
 // Forward then backward cluster solve on `stream`: x1 = forward result (global
 // scratch), out = backward result.
-template <typename T>
+template <typename T, bool kTrans = false>
 inline void launch_cluster_solve(int n, const T *LU, const int *perm, const int *flags,
                                  const GArgs &ga, T *x1, T *out, int *err, cudaStream_t stream) {
     const size_t bytes = cluster_smem_bytes<T>(n);
@@ -265,9 +270,9 @@ inline void launch_cluster_solve(int n, const T *LU, const int *perm, const int 
     static bool attr_done = false;
     if (!attr_done) {
         const int maxb = (int)cluster_smem_bytes<T>(kMaxSolveN);
-        D4_CUDA_OK(cudaFuncSetAttribute(k_trsv_cluster<true, T>,
+        D4_CUDA_OK(cudaFuncSetAttribute(k_trsv_cluster<true, T, kTrans>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, maxb));
-        D4_CUDA_OK(cudaFuncSetAttribute(k_trsv_cluster<false, T>,
+        D4_CUDA_OK(cudaFuncSetAttribute(k_trsv_cluster<false, T, kTrans>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, maxb));
         attr_done = true;
     }
@@ -284,11 +289,11 @@ inline void launch_cluster_solve(int n, const T *LU, const int *perm, const int 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const T *none = nullptr;
-    D4_CUDA_OK(cudaLaunchKernelEx(&cfg, k_trsv_cluster<true, T>, n, LU, perm, flags, ga, x1, none,
-                                  err));
+    D4_CUDA_OK(cudaLaunchKernelEx(&cfg, k_trsv_cluster<true, T, kTrans>, n, LU, perm, flags, ga, x1,
+                                  none, err));
     check_launch("k_trsv_cluster<fwd>");
-    D4_CUDA_OK(cudaLaunchKernelEx(&cfg, k_trsv_cluster<false, T>, n, LU, perm, flags, ga, out,
-                                  (const T *)x1, err));
+    D4_CUDA_OK(cudaLaunchKernelEx(&cfg, k_trsv_cluster<false, T, kTrans>, n, LU, perm, flags, ga,
+                                  out, (const T *)x1, err));
     check_launch("k_trsv_cluster<bwd>");
 }
 
