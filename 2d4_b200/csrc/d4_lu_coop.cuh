@@ -5,6 +5,7 @@
 #include <type_traits>
 
 #include "d4_internal.h"
+#include "d4_qdiv.cuh"
 
 namespace d4 {
 namespace coop {
@@ -94,11 +95,12 @@ __device__ __forceinline__ int src_row(int r, const int *sa, const int *sb, int 
 // Diagonal block of the pass, in every CTA, by all its threads on shared
 // memory (two block barriers per column).  Pre-division values go to Q (CTA
 // 0), flags into the returned mask (meaningful in thread 0's and the column
-// owners' copies; they are OR-ed over the CTA).
+// owners' copies; they are OR-ed over the CTA).  A spare thread stores each
+// pivot's correctly rounded reciprocal in rs, for the rows below.
 template <typename T>
 __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[NB + 1],
-                                            int k0, int kw, const int *sa, const int *sb, int ns,
-                                            unsigned skip, bool write_q) {
+                                            T *rs, int k0, int kw, const int *sa, const int *sb,
+                                            int ns, unsigned skip, bool write_q) {
     const int n = a.n;
     const int tid = threadIdx.x;
     unsigned msk = 0;
@@ -112,6 +114,7 @@ __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[N
     for (int k = 0; k < kw; ++k) {
         const T d = s[k][k];
         const bool sk = (skip >> k) & 1u;
+        if (tid == NB) rs[k] = qdiv::recip(d);
         if (tid < NB) {
             const int r = tid;
             if (write_q && r >= k && r < kw) Q[(size_t)(k0 + r) + (size_t)k * n] = s[r][k];
@@ -142,11 +145,13 @@ __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[N
 // Rows below the diagonal block, 8 lanes per row: lane q of a group owns the
 // columns q, q+8, q+16, q+24 of its row in registers.  Column k's owner divides
 // and broadcasts the multiplier by shuffle; every lane then updates its own
-// columns j > k.  Each entry keeps the oracle's update order.  Pre-division
+// columns j > k.  Each entry keeps the oracle's update order; the multiplier
+// is the IEEE quotient, formed from the pivot's reciprocal (rs).  Pre-division
 // values to Q, multipliers to A, flags into the returned mask.
 template <int KW, typename T>
 __device__ __forceinline__ unsigned rows_below_t(const CoopArgs<T> &a, T *Q,
-                                                 const T (*s)[NB + 1], int r_pos, int sr,
+                                                 const T (*s)[NB + 1], const T *rs, int r_pos,
+                                                 int sr,
                                                  int k0, unsigned skip, bool active) {
     const int n = a.n;
     const int lane = threadIdx.x & 31, q = lane & 7, gbase = lane & ~7;
@@ -167,7 +172,7 @@ __device__ __forceinline__ unsigned rows_below_t(const CoopArgs<T> &a, T *Q,
             T l = 0.0;
             if (q == own) {
                 if (active && fabs(v) > fabs(d)) msk |= 1u << k;
-                l = v / d;
+                l = qdiv::div(v, d, rs[k]);
                 c[slot] = l;
             }
             l = __shfl_sync(0xffffffffu, l, gbase + own);
@@ -192,7 +197,7 @@ __device__ __forceinline__ unsigned rows_below_t(const CoopArgs<T> &a, T *Q,
 // Narrow last block (kw < 32): one thread per row, shared-memory row.
 template <typename T>
 __device__ __noinline__ unsigned rows_below_var(const CoopArgs<T> &a, T *Q,
-                                                const T (*s)[NB + 1], T *rowbuf,
+                                                const T (*s)[NB + 1], const T *rs, T *rowbuf,
                                                 int r_pos, int sr, int k0, int kw,
                                                 unsigned skip) {
     const int n = a.n;
@@ -205,7 +210,7 @@ __device__ __noinline__ unsigned rows_below_var(const CoopArgs<T> &a, T *Q,
         if (!((skip >> k) & 1u)) {
             const T d = s[k][k];
             if (fabs(v) > fabs(d)) msk |= 1u << k;
-            const T l = v / d;
+            const T l = qdiv::div(v, d, rs[k]);
             rv[k] = l;
             for (int j = k + 1; j < kw; ++j) {
                 const T u = s[k][j];
@@ -219,7 +224,7 @@ __device__ __noinline__ unsigned rows_below_var(const CoopArgs<T> &a, T *Q,
 
 template <typename T>
 __device__ __noinline__ unsigned rows_below(const CoopArgs<T> &a, T *Q,
-                                            const T (*s)[NB + 1], T *rowbuf, int k0,
+                                            const T (*s)[NB + 1], const T *rs, T *rowbuf, int k0,
                                             int kw, const int *sa, const int *sb, int ns,
                                             unsigned skip) {
     const int n = a.n;
@@ -233,12 +238,12 @@ __device__ __noinline__ unsigned rows_below(const CoopArgs<T> &a, T *Q,
             const bool active = g < rows;
             const int r_pos = k0 + kw + (active ? g : 0);
             const int sr = active ? src_row(r_pos, sa, sb, ns) : 0;
-            msk |= rows_below_t<NB, T>(a, Q, s, r_pos, sr, k0, skip, active);
+            msk |= rows_below_t<NB, T>(a, Q, s, rs, r_pos, sr, k0, skip, active);
         }
     } else {
         for (int g = blockIdx.x * kThreads + threadIdx.x; g < rows; g += gridDim.x * kThreads) {
             const int r_pos = k0 + kw + g;
-            msk |= rows_below_var(a, Q, s, rowbuf, r_pos, src_row(r_pos, sa, sb, ns), k0, kw,
+            msk |= rows_below_var(a, Q, s, rs, rowbuf, r_pos, src_row(r_pos, sa, sb, ns), k0, kw,
                                   skip);
         }
     }
@@ -343,6 +348,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     extern __shared__ __align__(16) unsigned char rowbuf_raw[];
     T *rowbuf = reinterpret_cast<T *>(rowbuf_raw);  // kThreads rows of NB+1 entries
     __shared__ T s[NB][NB + 1];           // diagonal block (rows = positions k0..k0+31)
+    __shared__ T rs[NB];                  // RN(1 / pivot) of the block's columns
     __shared__ T Ls[NB][64 + 1];          // update: L21 tile
     __shared__ T Us[NB][64 + 1];          // update: U12 tile
     __shared__ int sa[NB], sb[NB];        // swap list of the block (positions)
@@ -406,8 +412,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             const unsigned skip = skip_mask;
             if (tid == 0) cta_mask = 0;
             // diagonal block, redundantly in every CTA (warp 0), then the rows below
-            unsigned my_mask = diag_block(a, Q, s, k0, kw, sa, sb, ns, skip, cta == 0);
-            my_mask |= rows_below(a, Q, s, rowbuf, k0, kw, sa, sb, ns, skip);
+            unsigned my_mask = diag_block(a, Q, s, rs, k0, kw, sa, sb, ns, skip, cta == 0);
+            my_mask |= rows_below(a, Q, s, rs, rowbuf, k0, kw, sa, sb, ns, skip);
             if (my_mask) atomicOr(&cta_mask, my_mask);
             __syncthreads();
             if (tid == 0 && cta_mask) atomicOr(&a.mask[pass], cta_mask);

@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "d4_internal.h"
+#include "d4_qdiv.cuh"
 
 namespace d4 {
 namespace trsv {
@@ -184,6 +185,10 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
 #pragma unroll
         for (int k = 0; k < 32; ++k) dt[lane][k] = tl[k];
         __syncwarp();
+        // this lane's divisor and its reciprocal, formed before the chain
+        // (the quotient in the chain is still the IEEE one)
+        const T dmine = dt[lane][lane];
+        const T rmine = qdiv::recip(dmine);
         const int napply = kFwd ? b : nblk - 1 - b;
         for (int s = 0; s < napply; ++s) {
             const int kb = kFwd ? s : nblk - 1 - s;
@@ -229,14 +234,14 @@ __global__ void __launch_bounds__(32 * kClusterMaxWarps) k_trsv_cluster(
         if (kFwd) {
 #pragma unroll
             for (int k = 0; k < 32; ++k) {
-                if (kTrans && k < kw && lane == k) xi = xi / dt[k][k];
+                if (kTrans && k < kw && lane == k) xi = qdiv::div(xi, dmine, rmine);
                 const T t = __shfl_sync(0xffffffffu, xi, k);
                 if (k < kw && lane > k && t != T(0)) xi = xi - dt[lane][k] * t;
             }
         } else {
 #pragma unroll
             for (int k = 31; k >= 0; --k) {
-                if (!kTrans && k < kw && lane == k) xi = xi / dt[k][k];
+                if (!kTrans && k < kw && lane == k) xi = qdiv::div(xi, dmine, rmine);
                 const T t = __shfl_sync(0xffffffffu, xi, k);
                 if (k < kw && lane < k && t != T(0)) xi = xi - dt[lane][k] * t;
             }
