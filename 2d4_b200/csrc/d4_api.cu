@@ -297,6 +297,7 @@ static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
         if (fl[k * d4::kFlagCount + d4::kFlagBarrierTimeout])
             throw d4::StateError("LU grid barrier timed out");
         singular |= fl[k * d4::kFlagCount + d4::kFlagSingular] != 0;
+        d4::count_lu(c, fl + k * d4::kFlagCount);
     }
     // the last factorisation's flags stand for the context's (d4_solve etc.)
     D4_CUDA_OK(cudaMemcpyAsync(c.flags, L3.flags, sizeof(int) * d4::kFlagCount,
@@ -1061,6 +1062,15 @@ int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long lo
     *iterations = c->sp_iters;
     *fallbacks = c->sp_fallbacks;
     *nnz = c->sp_nnz;
+    return D4_OK;
+}
+
+int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long long *swaps) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !factorizations || !passes || !swaps) return D4_ERR_ARG;
+    *factorizations = c->lu_count;
+    *passes = c->lu_passes;
+    *swaps = c->lu_swaps;
     return D4_OK;
 }
 

@@ -22,6 +22,8 @@ enum FlagSlot {
     kFlagNeedPivot = 0,  // fast LU met |a_ik| > |a_kk| or a_kk == 0: partial pivoting would swap
     kFlagSingular = 1,   // pivoted LU met an exact zero pivot
     kFlagBarrierTimeout = 2,  // a bounded grid-barrier wait gave up
+    kFlagPasses = 3,     // cooperative LU: passes over the column blocks
+    kFlagSwaps = 4,      // cooperative LU: row swaps (pivots off the diagonal)
     kFlagCount = 8
 };
 
@@ -127,6 +129,8 @@ struct Ctx {
     double *sp_val = nullptr, *sp_dinv = nullptr, *sp_V = nullptr, *sp_z = nullptr,
            *sp_w = nullptr, *sp_g = nullptr, *sp_x = nullptr, *sp_part = nullptr;
     long long sp_solves = 0, sp_iters = 0, sp_fallbacks = 0;
+    // cooperative LU counters (d4_lu_stats)
+    long long lu_count = 0, lu_passes = 0, lu_swaps = 0;
 
     // tabulated field (null: analytic field)
     double2 *tab = nullptr;
@@ -191,6 +195,13 @@ int factor64(Ctx &c);                 // d4_lu_coop64.cu
 void factor64_async(Ctx &c, const LuBufs &L, const double *A, int grid, cudaStream_t st,
                     cudaEvent_t after_copy);
 LuBufs primary_lu(Ctx &c);
+// Adds one factorisation's pass and swap counts (its flag words) to the
+// context's counters.
+inline void count_lu(Ctx &c, const int *fl) {
+    ++c.lu_count;
+    c.lu_passes += fl[kFlagPasses];
+    c.lu_swaps += fl[kFlagSwaps];
+}
 int coop_grid_size(int n);            // CTAs of the cooperative LU (-1: n too large)
 enum GMode { kGBig = 0, kGHalf = 1, kGNewton = 2 };
 // g built from (gmode, hval, dvec, s_end, s_init, x_new, x_old); solve; out = base - dx.

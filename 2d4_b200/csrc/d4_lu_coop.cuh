@@ -37,7 +37,7 @@ struct CoopArgs {
     unsigned *mask;  // one word per pass (zeroed before the launch): flagged columns
     int *perm;       // n: original row of each position (receives the row swaps)
     int *piv;        // n pivot rows
-    int *flags;      // kFlagSingular, kFlagBarrierTimeout
+    int *flags;      // kFlagSingular, kFlagBarrierTimeout, kFlagPasses, kFlagSwaps
     unsigned *bar;   // grid barrier: [0] arrivals, [kGenWord] generation
 };
 
@@ -395,7 +395,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     }
     grid_barrier(a.bar, a.flags, gen, &dead_s);
 
-    int pass = 0;  // global pass counter: mask word, and Q buffer by parity
+    int swaps = 0;  // thread 0: row swaps so far
+    int pass = 0;   // global pass counter: mask word, and Q buffer by parity
     for (int kb = 0; kb < nblk; ++kb) {
         const int k0 = kb * NB, kw = min(NB, n - k0);
         if (tid == 0) {
@@ -473,6 +474,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
         }
         // ---------------------------------------------------------- finish
         const int ns = ns_s;
+        swaps += ns;
         if (cta == 0) {
             for (int t = tid; t < NB * NB; t += kThreads) {
                 const int r = t % NB, k = t / NB;
@@ -662,6 +664,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             // never read from P0 (positions >= nk0 only)
         }
         grid_barrier(a.bar, a.flags, gen, &dead_s);
+    }
+    if (cta == 0 && tid == 0) {
+        a.flags[kFlagPasses] = pass;
+        a.flags[kFlagSwaps] = swaps;
     }
     if (kTc) {
         tc::fence_before();

@@ -318,6 +318,7 @@ int factor32(Ctx &c) {
                                cudaMemcpyDeviceToHost, c.stream));
     D4_CUDA_OK(cudaStreamSynchronize(c.stream));
     if (c.h_flags[kFlagBarrierTimeout]) throw StateError("LU grid barrier timed out");
+    count_lu(c, c.h_flags);
     c.factor_singular = c.h_flags[kFlagSingular] != 0;
     c.factor_pivoted = 0;
     return c.factor_singular ? D4_WARN_SINGULAR : D4_OK;

@@ -337,6 +337,13 @@ class Engine:
         self._call("d4_solver_stats", *[C.byref(t) for t in v])
         return dict(zip(("solves", "iterations", "fallbacks", "nnz"), [t.value for t in v]))
 
+    def lu_stats(self):
+        """Counters of the dense cooperative LU (d4_lu_stats): factorisations,
+        passes over their 32-column blocks, row swaps."""
+        v = [C.c_longlong() for _ in range(3)]
+        self._call("d4_lu_stats", *[C.byref(t) for t in v])
+        return dict(zip(("factorizations", "passes", "swaps"), [t.value for t in v]))
+
     def positions(self):
         x = np.empty(self.n)
         y = np.empty(self.n)

@@ -245,11 +245,16 @@ def mixed_vs_fp64(pkg, steps=8, warmup=2, n=4096, seed=1002, tau=0.1):
         eng = pkg.Engine(sd)
         eng.advance(warmup)
         eng.profile(True)
+        lu0 = eng.lu_stats()
         r = eng.advance(steps)
+        lu1 = eng.lu_stats()
         prof = eng.profile_read()
+        nlu = max(lu1["factorizations"] - lu0["factorizations"], 1)
         out[name] = dict(value=n * steps / r.device_seconds, attempts=int(r.attempts),
                          failed=int(r.failed_steps), x=eng.positions()[0],
-                         ms_per_call={k: round(v[0] / max(v[1], 1), 3) for k, v in prof.items()})
+                         ms_per_call={k: round(v[0] / max(v[1], 1), 3) for k, v in prof.items()},
+                         lu_passes_per_block=(lu1["passes"] - lu0["passes"]) / (nlu * -(-n // 32)),
+                         lu_swaps=(lu1["swaps"] - lu0["swaps"]) / nlu)
         eng.close()
     d, _, _, _ = pkg.dconf.conf_compare(out["mixed"]["x"], y, out["fp64"]["x"], y)
     return {"n": n, "tau_ext": tau, "steps": steps, "warmup": warmup,
@@ -260,7 +265,10 @@ def mixed_vs_fp64(pkg, steps=8, warmup=2, n=4096, seed=1002, tau=0.1):
             "attempts": [out["fp64"]["attempts"], out["mixed"]["attempts"]],
             "max_position_diff_vs_fp64": d,
             "fp64_ms_per_call": out["fp64"]["ms_per_call"],
-            "mixed_ms_per_call": out["mixed"]["ms_per_call"]}
+            "mixed_ms_per_call": out["mixed"]["ms_per_call"],
+            "lu_passes_per_block": [out["fp64"]["lu_passes_per_block"],
+                                    out["mixed"]["lu_passes_per_block"]],
+            "lu_swaps_per_factorization": [out["fp64"]["lu_swaps"], out["mixed"]["lu_swaps"]]}
 
 
 def cutoff_leg(pkg, steps=6, warmup=1, n=4096, seed=1002, tau=0.1, u=6.4):
@@ -461,6 +469,7 @@ def main():
 
     clocks = ClockSampler(local)
     launches0 = lib.d4_kernel_launches()
+    lu0 = eng.lu_stats()
     eng.profile(True)
     clocks.start()
     barrier()
@@ -475,6 +484,7 @@ def main():
     barrier()
     clk = clocks.stop()
     launches = lib.d4_kernel_launches() - launches0
+    lu1 = eng.lu_stats()
     prof = eng.profile_read()
     eng.profile(False)
 
@@ -528,6 +538,11 @@ def main():
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "kernel_ms": {k: v[0] for k, v in prof.items()},
             "kernel_calls": {k: v[1] for k, v in prof.items()}}
+    nlu = lu1["factorizations"] - lu0["factorizations"]
+    if nlu > 0:
+        line["lu"] = {"factorizations": nlu,
+                      "passes_per_block": (lu1["passes"] - lu0["passes"]) / (nlu * -(-n // 32)),
+                      "swaps_per_factorization": (lu1["swaps"] - lu0["swaps"]) / nlu}
     if ws == 1 and not args.no_mixed:
         try:
             line["mixed_vs_fp64"] = mixed_vs_fp64(pkg)

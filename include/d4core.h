@@ -227,6 +227,12 @@ int d4_profile_read(void *ctx, double *ms, long long *calls);
 int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long long *fallbacks,
                     long long *nnz);
 
+/* Counters of the dense cooperative LU (plain and mixed forms): factorisations
+ * run, passes over their 32-column blocks summed over them (one per block,
+ * plus one per row swap found after a block's optimistic pass), and row swaps
+ * (pivots off the diagonal).  No counterpart in the reference. */
+int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long long *swaps);
+
 /* Batched ensemble of independent systems: the many-realisation statistics
  * workload, where the reference runs one system per process
  * (src/simulation.cpp:30-281).  FP64 form, analytic field, dense LU; every

@@ -135,6 +135,11 @@ def test_factor_solve_pivoted_exact(pkg, restated, n):
     assert (piv != np.arange(m)).any()
     assert np.array_equal(dx, dx_o)
     assert np.abs(a @ dx - g).max() < 1e-9
+    # counters: every swap is the oracle's, and costs one extra pass over its block
+    st = e.lu_stats()
+    swaps = int((piv != np.arange(m)).sum())
+    assert st["factorizations"] == 1 and st["swaps"] == swaps
+    assert st["passes"] == -(-m // 32) + swaps
 
 
 def test_factor_singular(pkg, restated):
