@@ -111,9 +111,11 @@ void free_all(Ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
+    const d4::Mix32Bufs &B = c->m32b;
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
-                  c->xw2_b, c->dx_b};
+                  c->xw2_b, c->dx_b, B.A32, B.LU32, B.P0, B.Q, B.mask, B.bar, B.perm, B.piv,
+                  B.g, B.r, B.dx, B.c32, B.w1, B.resid, c->m_vacc_b};
     for (void *b : ob)
         if (b) cudaFree(b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -307,11 +309,154 @@ static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
     *singular_out = singular;
 }
 
+// Worst refined residual max|r| / max|g| over a ring of 8 (max |r|, max |g|)
+// pairs (as ordered bits of non-negatives), 0 where nothing was recorded.
+static double worst_refined(const unsigned long long *rb) {
+    double worst = 0;
+    for (int k = 0; k < 8; ++k) {
+        double r, g;
+        std::memcpy(&r, &rb[2 * k], 8);
+        std::memcpy(&g, &rb[2 * k + 1], 8);
+        if (g > 0) worst = std::max(worst, r / g);
+    }
+    return worst;
+}
+
+// The mixed form's stages I-IV with stage I on a second stream, as
+// attempt_overlap: stage I copies A1 into its own FP32 matrix (the one its
+// refinement multiplies) while factorising it, and runs its two refined solves
+// and its stress sweep on stream_b with its own buffers; stages II and III run
+// on the context's stream.  Every operation is the sequential attempt's, so
+// the results are identical.  *refine_out: the worst refined residual of the
+// attempt's six solves.
+static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out,
+                                  double *refine_out) {
+    using d4::ProfScope;
+    const d4_protocol &pr = c.p.protocol;
+    const double t1 = t0 + h, th = t0 + h / 2;
+    const int n = c.n;
+    d4::Mix32Bufs B1 = c.m32b, B2 = d4::primary_mix32(c), B3 = d4::primary_mix32(c);
+    B1.flags = c.flags3;
+    B2.flags = c.flags3 + d4::kFlagCount;
+    B3.flags = c.flags3 + 2 * d4::kFlagCount;
+    const int half = std::max(1, c.lu32_grid / 2);
+    cudaStream_t sa = c.stream, sb = c.stream_b;
+    {
+        ProfScope ps(c, D4_CAT_JACOBIAN);
+        d4::jacobian32(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t1), c.v_init, c.speed);
+    }
+    D4_CUDA_OK(cudaMemcpyAsync(c.dvec_b, c.dvec, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
+    D4_CUDA_OK(cudaMemcpyAsync(c.speed_b, c.speed, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
+    D4_CUDA_OK(cudaEventRecord(c.ev_fork, sa));
+    D4_CUDA_OK(cudaStreamWaitEvent(sb, c.ev_fork, 0));
+    // stage I on stream_b
+    {
+        ProfScope ps(c, D4_CAT_FACTOR, sb);
+        d4::factor32_async(c, B1, c.A32, true, half, sb, c.ev_copy);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE, sb);
+        d4::solve_update32_with(c, B1, c.dvec_b, c.dx_b, sb, d4::kGBig, h, c.speed_b, c.v_init,
+                                nullptr, nullptr, c.x0, c.xb);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS, sb);
+        d4::speeds32_with(c, c.m_vacc_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE, sb);
+        d4::solve_update32_with(c, B1, c.dvec_b, c.dx_b, sb, d4::kGNewton, h, c.speed2_b,
+                                c.v_init, c.xb, c.x0, c.xb, c.xb);
+    }
+    D4_CUDA_OK(cudaEventRecord(c.ev_join, sb));
+    // stage II on the context's stream, once A1 is copied
+    D4_CUDA_OK(cudaStreamWaitEvent(sa, c.ev_copy, 0));
+    {
+        ProfScope ps(c, D4_CAT_RESCALE);
+        d4::jacobian_from_prev32(c, (th - t0) / (t1 - t0));
+    }
+    {
+        ProfScope ps(c, D4_CAT_FACTOR);
+        d4::factor32_async(c, B2, c.A32, false, half, sa, nullptr);
+    }
+    d4::shift_speed64(c, c.speed, ext_stress(pr, th) - ext_stress(pr, t1));
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update32_with(c, B2, c.dvec, c.dx, sa, d4::kGHalf, h, c.speed, c.v_init, nullptr,
+                                nullptr, c.x0, c.xh);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS);
+        d4::speeds32(c, c.xh, c.y, ext_stress(pr, th), c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update32_with(c, B2, c.dvec, c.dx, sa, d4::kGNewton, h / 2, c.speed2, c.v_init,
+                                c.xh, c.x0, c.xh, c.xh);
+    }
+    // stage III
+    {
+        ProfScope ps(c, D4_CAT_JACOBIAN);
+        d4::jacobian32(c, c.xh, c.y, h / 2, ext_stress(pr, th), ext_stress(pr, t1), c.v_init2,
+                       c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_FACTOR);
+        d4::factor32_async(c, B3, c.A32, false, c.lu32_grid, sa, nullptr);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update32_with(c, B3, c.dvec, c.dx, sa, d4::kGHalf, h, c.speed2, c.v_init2,
+                                nullptr, nullptr, c.xh, c.x2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SPEEDS);
+        d4::speeds32(c, c.x2, c.y, ext_stress(pr, t1), c.speed2);
+    }
+    {
+        ProfScope ps(c, D4_CAT_SOLVE);
+        d4::solve_update32_with(c, B3, c.dvec, c.dx, sa, d4::kGNewton, h / 2, c.speed2,
+                                c.v_init2, c.x2, c.xh, c.x2, c.x2);
+    }
+    D4_CUDA_OK(cudaStreamWaitEvent(sa, c.ev_join, 0));
+    d4::error_ratio64(c, c.xb, c.x2);
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_red, c.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, sa));
+    D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.wave_err, sizeof(int) * 6, cudaMemcpyDeviceToHost, sa));
+    int fl[3 * d4::kFlagCount];
+    D4_CUDA_OK(cudaMemcpyAsync(fl, c.flags3, sizeof(fl), cudaMemcpyDeviceToHost, sa));
+    unsigned long long rb[2][16];
+    D4_CUDA_OK(cudaMemcpyAsync(rb[0], c.m_resid, sizeof(rb[0]), cudaMemcpyDeviceToHost, sa));
+    D4_CUDA_OK(cudaMemcpyAsync(rb[1], c.m32b.resid, sizeof(rb[1]), cudaMemcpyDeviceToHost, sa));
+    sync(c);
+    if (c.prof.on) d4::prof_collect(c);
+    check_async_errors(c);
+    int singular = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (fl[k * d4::kFlagCount + d4::kFlagBarrierTimeout])
+            throw d4::StateError("LU grid barrier timed out");
+        singular |= fl[k * d4::kFlagCount + d4::kFlagSingular] != 0;
+        d4::count_lu(c, fl + k * d4::kFlagCount);
+    }
+    // the last factorisation's flags stand for the context's (d4_solve etc.)
+    D4_CUDA_OK(cudaMemcpyAsync(c.flags, B3.flags, sizeof(int) * d4::kFlagCount,
+                               cudaMemcpyDeviceToDevice, sa));
+    D4_CUDA_OK(cudaMemsetAsync(c.m_resid, 0, sizeof(rb[0]), sa));
+    D4_CUDA_OK(cudaMemsetAsync(c.m32b.resid, 0, sizeof(rb[1]), sa));
+    c.factor_singular = fl[2 * d4::kFlagCount + d4::kFlagSingular] != 0;
+    c.factor_pivoted = 0;
+    *singular_out = singular;
+    *refine_out = std::max(worst_refined(rb[0]), worst_refined(rb[1]));
+}
+
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     if (c.overlap) {
         int singular = 0;
-        attempt_overlap(c, t0, h, &singular);
+        double refine = 0;
+        if (c.p.precision == D4_PREC_MIXED)
+            attempt_overlap_mixed(c, t0, h, &singular, &refine);
+        else
+            attempt_overlap(c, t0, h, &singular);
         const int idx = (int)c.h_red[1];
         if (idx >= 0) c.selected_id = idx;
         res->ratio = c.h_red[0] / c.dipole_prec_sq;
@@ -319,7 +464,7 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
         res->accepted = res->ratio < 1;
         res->singular = singular;
         res->pivoted = 0;
-        res->refine_residual = 0;
+        res->refine_residual = refine;
         return D4_OK;
     }
     using d4::ProfScope;
@@ -419,14 +564,7 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     if (mixed) {
         unsigned long long rb[16];
         D4_CUDA_OK(cudaMemcpy(rb, c.m_resid, sizeof(rb), cudaMemcpyDeviceToHost));
-        double worst = 0;
-        for (int k = 0; k < 8; ++k) {
-            double r, g;
-            std::memcpy(&r, &rb[2 * k], 8);
-            std::memcpy(&g, &rb[2 * k + 1], 8);
-            if (g > 0) worst = std::max(worst, r / g);
-        }
-        res->refine_residual = worst;
+        res->refine_residual = worst_refined(rb);
         D4_CUDA_OK(cudaMemset(c.m_resid, 0, sizeof(rb)));
     }
     return D4_OK;
@@ -606,25 +744,46 @@ int d4_create(void **out, int n, const d4_params *p) {
         }
         c->use_gmres = d4::gmres_selected(*c) ? 1 : 0;
         if (c->use_gmres) d4::sparse_alloc(*c);
-        if (!mixed && !c->use_gmres) {
-            // stage I's own stream and buffers (attempt_overlap)
+        if (!c->use_gmres) {
+            // stage I's own stream and buffers (attempt_overlap, attempt_overlap_mixed)
             c->overlap = 1;
             D4_CUDA_OK(cudaStreamCreateWithFlags(&c->stream_b, cudaStreamNonBlocking));
             D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
             D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming));
             D4_CUDA_OK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
-            dalloc(&c->lub.LU, nn);
-            dalloc(&c->lub.P0, (size_t)n * 32);
-            dalloc(&c->lub.Q, (size_t)n * 64);
-            dalloc(&c->lub.mask, (size_t)c->lu_mask_words);
-            dalloc(&c->lub.bar, 64);
-            dalloc(&c->lub.perm, (size_t)n);
-            dalloc(&c->lub.piv, (size_t)n);
             dalloc(&c->flags3, (size_t)3 * d4::kFlagCount);
-            dalloc(&c->F_b, nn);
             double **bv[] = {&c->dvec_b, &c->speed_b, &c->speed2_b, &c->xw1_b, &c->xw2_b,
                              &c->dx_b};
             for (double **v : bv) dalloc(v, (size_t)n);
+            if (!mixed) {
+                dalloc(&c->lub.LU, nn);
+                dalloc(&c->lub.P0, (size_t)n * 32);
+                dalloc(&c->lub.Q, (size_t)n * 64);
+                dalloc(&c->lub.mask, (size_t)c->lu_mask_words);
+                dalloc(&c->lub.bar, 64);
+                dalloc(&c->lub.perm, (size_t)n);
+                dalloc(&c->lub.piv, (size_t)n);
+                dalloc(&c->F_b, nn);
+            } else {
+                d4::Mix32Bufs &B = c->m32b;
+                dalloc(&B.A32, nn);
+                dalloc(&B.LU32, nn);
+                dalloc(&B.P0, (size_t)n * 32);
+                dalloc(&B.Q, (size_t)n * 64);
+                dalloc(&B.mask, (size_t)c->lu_mask_words);
+                dalloc(&B.bar, 64);
+                dalloc(&B.perm, (size_t)n);
+                dalloc(&B.piv, (size_t)n);
+                dalloc(&B.g, (size_t)n);
+                dalloc(&B.r, (size_t)n);
+                dalloc(&B.dx, (size_t)n);
+                dalloc(&B.c32, (size_t)n);
+                dalloc(&B.w1, (size_t)n);
+                dalloc(&B.resid, 16);
+                D4_CUDA_OK(cudaMemset(B.resid, 0, sizeof(unsigned long long) * 16));
+                B.resid_count = &c->m_resid_count_b;
+                dalloc(&c->m_vacc_b, (size_t)n);
+            }
         }
         d4::reset_tol64(*c);
         sync(*c);
@@ -1062,6 +1221,13 @@ int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long lo
     *iterations = c->sp_iters;
     *fallbacks = c->sp_fallbacks;
     *nnz = c->sp_nnz;
+    return D4_OK;
+}
+
+int d4_set_overlap(void *ctx, int enable) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    c->overlap = (enable && c->stream_b) ? 1 : 0;  // the second stream exists unless GMRES
     return D4_OK;
 }
 

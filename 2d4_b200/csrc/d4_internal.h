@@ -38,6 +38,19 @@ struct LuBufs {
     int *flags = nullptr, *perm = nullptr, *piv = nullptr;
 };
 
+// Buffers of one FP32 factorisation and its refined solves (mixed form): the
+// matrix the refinement's residual multiplies, the factors and the pivot
+// bookkeeping, the refinement vectors and the ring of residual maxima.
+struct Mix32Bufs {
+    float *A32 = nullptr, *LU32 = nullptr, *P0 = nullptr, *Q = nullptr;
+    unsigned *mask = nullptr, *bar = nullptr;
+    int *flags = nullptr, *perm = nullptr, *piv = nullptr;
+    double *g = nullptr, *r = nullptr, *dx = nullptr;
+    float *c32 = nullptr, *w1 = nullptr;
+    unsigned long long *resid = nullptr;  // 8 pairs (max |r|, max |g|)
+    int *resid_count = nullptr;           // host: next slot of resid
+};
+
 // Buffers of the solves of one stage chain: the weights read by the
 // residual, the forward-solve scratch and the correction.
 struct SolveBufs {
@@ -151,6 +164,10 @@ struct Ctx {
     double *F_b = nullptr, *dvec_b = nullptr, *speed_b = nullptr, *speed2_b = nullptr,
            *xw1_b = nullptr, *xw2_b = nullptr, *dx_b = nullptr;
     int *flags3 = nullptr;  // 3 x kFlagCount
+    // mixed form: stage I's FP32 buffers and pair-sum scratch
+    Mix32Bufs m32b;
+    double *m_vacc_b = nullptr;
+    int m_resid_count_b = 0;
 
     RunState rs;
     Prof prof;
@@ -221,6 +238,21 @@ void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v);
 void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
                 double *v_a, double *v_b);
 void jacobian_from_prev32(Ctx &c, double factor);
+// The context's own FP32 buffers (stages II and III, and the sequential attempt).
+Mix32Bufs primary_mix32(Ctx &c);
+// FP32 factorisation into B.LU32 on `st` with `grid` CTAs, without waiting;
+// with copy_matrix, A is also copied into B.A32 (the refinement's matrix).
+// `after_copy` (may be null) is recorded once A has been copied.
+void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix, int grid,
+                    cudaStream_t st, cudaEvent_t after_copy);
+// solve_update32 with explicit buffers, weights, correction output and stream.
+void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
+                         cudaStream_t st, int gmode, double hval, const double *s_end,
+                         const double *s_init, const double *x_new, const double *x_old,
+                         const double *base, double *out);
+// speeds32 with its own pair-sum scratch on `st`.
+void speeds32_with(Ctx &c, double *vacc, cudaStream_t st, const double *x, const double *y,
+                   double ext, double *v);
 int factor32(Ctx &c);
 int coop_grid_size32(int n);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,

@@ -259,13 +259,19 @@ static int pair_tiles(int n) {
     return T * (T + 1) / 2;
 }
 
-void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v) {
-    D4_CUDA_OK(cudaMemsetAsync(c.m_vacc, 0, sizeof(double) * c.n, c.stream));
+void speeds32_with(Ctx &c, double *vacc, cudaStream_t st, const double *x, const double *y,
+                   double ext, double *v) {
+    D4_CUDA_OK(cudaMemsetAsync(vacc, 0, sizeof(double) * c.n, st));
     Pair32Args a = pair32(c, x, y);
-    k_pairs32<false><<<pair_tiles(c.n), dim3(32, 8), 0, c.stream>>>(a);
+    a.vacc = vacc;
+    k_pairs32<false><<<pair_tiles(c.n), dim3(32, 8), 0, st>>>(a);
     check_launch("k_pairs32<speeds>");
-    k_speed_fin32<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_vacc, ext, v);
+    k_speed_fin32<<<nb(c.n, 256), 256, 0, st>>>(c.n, vacc, ext, v);
     check_launch("k_speed_fin32");
+}
+
+void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v) {
+    speeds32_with(c, c.m_vacc, c.stream, x, y, ext, v);
 }
 
 void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
@@ -292,28 +298,56 @@ void jacobian_from_prev32(Ctx &c, double factor) {
                                c.stream));
 }
 
-int factor32(Ctx &c) {
+Mix32Bufs primary_mix32(Ctx &c) {
+    Mix32Bufs B;
+    B.A32 = c.A32;
+    B.LU32 = c.LU32;
+    B.P0 = c.lu32_p0;
+    B.Q = c.lu32_q;
+    B.mask = c.lu_mask;
+    B.bar = c.lu_bar;
+    B.flags = c.flags;
+    B.perm = c.perm;
+    B.piv = c.piv;
+    B.g = c.m_g;
+    B.r = c.m_r;
+    B.dx = c.m_dx;
+    B.c32 = c.m_c32;
+    B.w1 = c.m_w1;
+    B.resid = c.m_resid;
+    B.resid_count = &c.m_resid_count;
+    return B;
+}
+
+void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix, int grid,
+                    cudaStream_t st, cudaEvent_t after_copy) {
     const int n = c.n;
-    D4_CUDA_OK(cudaMemsetAsync(c.flags, 0, sizeof(int) * kFlagCount, c.stream));
-    D4_CUDA_OK(cudaMemsetAsync(c.lu_bar, 0, sizeof(unsigned) * 64, c.stream));
-    D4_CUDA_OK(cudaMemsetAsync(c.lu_mask, 0, sizeof(unsigned) * c.lu_mask_words, c.stream));
-    D4_CUDA_OK(cudaMemcpyAsync(c.LU32, c.A32, sizeof(float) * (size_t)n * n,
-                               cudaMemcpyDeviceToDevice, c.stream));
+    const size_t bytes = sizeof(float) * (size_t)n * n;
+    D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
+    D4_CUDA_OK(cudaMemsetAsync(B.bar, 0, sizeof(unsigned) * 64, st));
+    D4_CUDA_OK(cudaMemsetAsync(B.mask, 0, sizeof(unsigned) * c.lu_mask_words, st));
+    D4_CUDA_OK(cudaMemcpyAsync(B.LU32, A, bytes, cudaMemcpyDeviceToDevice, st));
+    if (copy_matrix) D4_CUDA_OK(cudaMemcpyAsync(B.A32, A, bytes, cudaMemcpyDeviceToDevice, st));
+    if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
     coop::CoopArgs<float> a;
     a.n = n;
-    a.A = c.LU32;
-    a.P0 = c.lu32_p0;
-    a.Q = c.lu32_q;
-    a.mask = c.lu_mask;
-    a.piv = c.piv;
-    a.flags = c.flags;
-    a.bar = c.lu_bar;
-    a.perm = c.perm;
+    a.A = B.LU32;
+    a.P0 = B.P0;
+    a.Q = B.Q;
+    a.mask = B.mask;
+    a.piv = B.piv;
+    a.flags = B.flags;
+    a.bar = B.bar;
+    a.perm = B.perm;
     void *args[] = {(void *)&a};
     const void *kern = (const void *)coop::k_lu_coop<float>;
-    D4_CUDA_OK(cudaLaunchCooperativeKernel(kern, dim3(c.lu32_grid), dim3(coop::kThreads), args,
-                                           coop::kRowBufBytes<float>(), c.stream));
+    D4_CUDA_OK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(coop::kThreads), args,
+                                           coop::kRowBufBytes<float>(), st));
     check_launch("k_lu_coop<float>");
+}
+
+int factor32(Ctx &c) {
+    factor32_async(c, primary_mix32(c), c.A32, false, c.lu32_grid, c.stream, nullptr);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
                                cudaMemcpyDeviceToHost, c.stream));
     D4_CUDA_OK(cudaStreamSynchronize(c.stream));
@@ -337,42 +371,49 @@ int coop_grid_size32(int n) {
     return g < (n + coop::kThreads - 1) / coop::kThreads ? -1 : g;
 }
 
-// FP32 cluster solve with LU32: c = LU32^-1 r (r FP64 in, c FP32 out).
-static void solve32_once(Ctx &c, const double *r, float *out) {
+// FP32 cluster solve with B's factors: out = LU32^-1 r (r FP64 in, out FP32).
+static void solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const double *r,
+                         float *out) {
     trsv::GArgs g{};
     g.gmode = -1;
     g.g_in = r;
-    trsv::launch_cluster_solve<float>(c.n, c.LU32, c.perm, c.flags, g, c.m_w1, out, c.wave_err,
-                                      c.stream);
+    trsv::launch_cluster_solve<float>(c.n, B.LU32, B.perm, B.flags, g, B.w1, out, c.wave_err, st);
 }
 
-void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
-                    const double *x_new, const double *x_old, const double *base, double *out) {
+void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
+                         cudaStream_t st, int gmode, double hval, const double *s_end,
+                         const double *s_init, const double *x_new, const double *x_old,
+                         const double *base, double *out) {
     const int n = c.n;
     trsv::GArgs ga{};
     ga.gmode = gmode;
     ga.hval = hval;
-    ga.dvec = c.dvec;
+    ga.dvec = dvec;
     ga.s_end = s_end;
     ga.s_init = s_init;
     ga.x_new = x_new;
     ga.x_old = x_old;
-    k_ir_init<<<nb(n, 256), 256, 0, c.stream>>>(n, ga, c.m_g, c.m_r, c.m_dx);
+    k_ir_init<<<nb(n, 256), 256, 0, st>>>(n, ga, B.g, B.r, B.dx);
     check_launch("k_ir_init");
     const int chunk = 256;
     for (int it = 0; it < c.ir_iters; ++it) {
-        solve32_once(c, c.m_r, c.m_c32);
-        k_ir_accum<<<nb(n, 256), 256, 0, c.stream>>>(n, c.m_c32, c.m_g, c.m_dx, c.m_r);
+        solve32_once(c, B, st, B.r, B.c32);
+        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, B.c32, B.g, B.dx, B.r);
         check_launch("k_ir_accum");
-        k_gemv_sub32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, c.stream>>>(n, c.A32, c.m_dx, c.m_r,
-                                                                         chunk);
+        k_gemv_sub32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(n, B.A32, B.dx, B.r, chunk);
         check_launch("k_gemv_sub32");
     }
-    k_absmax2<<<64, 256, 0, c.stream>>>(n, c.m_r, c.m_g, c.m_resid + 2 * c.m_resid_count);
+    k_absmax2<<<64, 256, 0, st>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");
-    c.m_resid_count = (c.m_resid_count + 1) % 8;
-    k_ir_apply<<<nb(n, 256), 256, 0, c.stream>>>(n, c.m_dx, c.flags, base, out, c.dx);
+    *B.resid_count = (*B.resid_count + 1) % 8;
+    k_ir_apply<<<nb(n, 256), 256, 0, st>>>(n, B.dx, B.flags, base, out, dx_out);
     check_launch("k_ir_apply");
+}
+
+void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
+                    const double *x_new, const double *x_old, const double *base, double *out) {
+    solve_update32_with(c, primary_mix32(c), c.dvec, c.dx, c.stream, gmode, hval, s_end, s_init,
+                        x_new, x_old, base, out);
 }
 
 }  // namespace d4

@@ -264,6 +264,11 @@ class Engine:
         self._call("d4_advance", C.c_longlong(accepted_steps), C.byref(r))
         return r
 
+    def set_overlap(self, enable=True):
+        """Stage I on a second stream, concurrent with stages II-III (default),
+        or all stages in sequence (d4_set_overlap); identical results."""
+        self._call("d4_set_overlap", int(bool(enable)))
+
     # accepted-step recording and the differentiation of a replayed step sequence
     def record_steps(self, enable=True):
         self._call("d4_record_steps", int(bool(enable)))

@@ -257,6 +257,15 @@ int d4_ensemble_get_positions(void *ens, int k, double *x, double *y);
  * every entry, device_seconds = the CUDA-event span of this call. */
 int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res);
 
+/* Schedule of an attempt (dense plain and mixed forms): enable = 1 (the
+ * default) runs stage I, the big step, on a second stream concurrently with
+ * stages II and III; 0 runs the stages one after the other on the context's
+ * stream (for a caller sharing the GPU with other work).  Both give identical
+ * results.  Ignored by the cutoff GMRES path, which is always sequential.  No
+ * counterpart in the reference (src/simulation.cpp:88-164 runs the stages in
+ * sequence). */
+int d4_set_overlap(void *ctx, int enable);
+
 /* Recording of accepted steps: while enabled, d4_run and d4_advance append
  * each accepted step's start time and size (the t and h of
  * src/simulation.cpp:88-164) to the context's list.  enable = 1 clears the
