@@ -178,6 +178,18 @@ void read_async_errors(Ctx &c) {
     check_async_errors(c);
 }
 
+// Grid split of an attempt's two concurrent cooperative factorisations:
+// stage I's chain (one LU, two solves, one sweep) is the shorter one, so it
+// gets 40% of the co-resident CTAs and stage II's factorisation the rest.
+// Neither gets fewer than one thread per row (n / 256 CTAs), as the full
+// grid's size check requires.
+static void stage_split(int grid, int n, int &g1, int &g2) {
+    const int need = (n + 255) / 256;
+    g1 = std::max(need, grid * 2 / 5);
+    g2 = grid - g1;
+    if (g2 < need) g1 = g2 = std::max(1, grid / 2);
+}
+
 // Stages I-IV with stage I on a second stream (FP64 dense form).  Stage I
 // (the big step: LU of A1, two solves, one stress sweep) feeds only the error
 // ratio, and stage II starts from the unfactored A1, so once A1 is copied into
@@ -206,7 +218,8 @@ static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
     Sb.xw1 = c.xw1_b;
     Sb.xw2 = c.xw2_b;
     Sb.dx = c.dx_b;
-    const int half = std::max(1, c.lu_grid / 2);
+    int g1, g2;
+    stage_split(c.lu_grid, n, g1, g2);
     cudaStream_t sa = c.stream, sb = c.stream_b;
     {
         ProfScope ps(c, D4_CAT_JACOBIAN);
@@ -219,7 +232,7 @@ static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
     // stage I on stream_b
     {
         ProfScope ps(c, D4_CAT_FACTOR, sb);
-        d4::factor64_async(c, L1, c.A, half, sb, c.ev_copy);
+        d4::factor64_async(c, L1, c.A, g1, sb, c.ev_copy);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE, sb);
@@ -244,7 +257,7 @@ static void attempt_overlap(Ctx &c, double t0, double h, int *singular_out) {
     }
     {
         ProfScope ps(c, D4_CAT_FACTOR);
-        d4::factor64_async(c, L2, c.A, half, sa, nullptr);
+        d4::factor64_async(c, L2, c.A, g2, sa, nullptr);
     }
     d4::shift_speed64(c, c.speed, ext_stress(pr, th) - ext_stress(pr, t1));
     {
@@ -339,7 +352,8 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     B1.flags = c.flags3;
     B2.flags = c.flags3 + d4::kFlagCount;
     B3.flags = c.flags3 + 2 * d4::kFlagCount;
-    const int half = std::max(1, c.lu32_grid / 2);
+    int g1, g2;
+    stage_split(c.lu32_grid, n, g1, g2);
     cudaStream_t sa = c.stream, sb = c.stream_b;
     {
         ProfScope ps(c, D4_CAT_JACOBIAN);
@@ -352,7 +366,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     // stage I on stream_b
     {
         ProfScope ps(c, D4_CAT_FACTOR, sb);
-        d4::factor32_async(c, B1, c.A32, true, half, sb, c.ev_copy);
+        d4::factor32_async(c, B1, c.A32, true, g1, sb, c.ev_copy);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE, sb);
@@ -377,7 +391,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     }
     {
         ProfScope ps(c, D4_CAT_FACTOR);
-        d4::factor32_async(c, B2, c.A32, false, half, sa, nullptr);
+        d4::factor32_async(c, B2, c.A32, false, g2, sa, nullptr);
     }
     d4::shift_speed64(c, c.speed, ext_stress(pr, th) - ext_stress(pr, t1));
     {
