@@ -487,6 +487,8 @@ struct HostInst {
     double strain = 0;
     int selected_id = 0;
     bool started = false;
+    long long aval_count = 0;  // avalanche detection (src/simulation.cpp:184-199)
+    bool in_aval = false;
 };
 
 struct Ensemble {
@@ -507,6 +509,7 @@ struct Ensemble {
     std::vector<int> act, pre_pair, pre_row, pre_mat;
     int solve_smem = 0;
     long long launches = 0;
+    long long vtot = 0;  // entries of each per-dislocation vector pool
 };
 
 void check(const char *name) {
@@ -607,6 +610,7 @@ bool interrupted(const Ensemble &E, const HostInst &h) {
     if (p.time_limit >= 0 && h.sim_time > p.time_limit) return true;
     if (p.strain_increase_limit >= 0 && h.strain > p.strain_increase_limit) return true;
     if (p.step_count_limit >= 0 && h.ok > p.step_count_limit) return true;
+    if (p.avalanche_limit >= 0 && h.aval_count > p.avalanche_limit) return true;
     return false;
 }
 
@@ -674,6 +678,7 @@ int d4_ensemble_create(void **out, int count, const int *n, const d4_params *p) 
             moff += (long long)n[k] * n[k];
             smax = std::max<long long>(smax, n[k]);
         }
+        E->vtot = voff;
         for (int v = 0; v < kNumVec; ++v) {
             D4_CUDA_OK(cudaMalloc((void **)&E->P.v[v], sizeof(double) * voff));
             D4_CUDA_OK(cudaMemsetAsync(E->P.v[v], 0, sizeof(double) * voff, E->stream));
@@ -851,6 +856,28 @@ int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res) {
                 double hn = 0.9 * hh * std::min(2., std::pow(r, -1. / 6));
                 if (p.max_stepsize > 0 && p.max_stepsize < hn) hn = p.max_stepsize;
                 h.step_size = hn;
+            }
+            if (p.avalanche_limit >= 0) {
+                // the accepted instances' mean |v| at the half-step position
+                // (v_init2), summed on the host in index order as d4_run does,
+                // drives the same two-state avalanche counter
+                std::vector<double> v2(E->vtot);
+                D4_CUDA_OK(cudaMemcpyAsync(v2.data(), E->P.v[kVI2], sizeof(double) * E->vtot,
+                                           cudaMemcpyDeviceToHost, E->stream));
+                D4_CUDA_OK(cudaStreamSynchronize(E->stream));
+                for (int k : active) {
+                    if (!acc[k]) continue;
+                    HostInst &h = E->hi[k];
+                    const Inst &in = E->hins[k];
+                    double sum = 0;
+                    for (int i = 0; i < in.n; ++i) sum = sum + std::fabs(v2[in.voff + i]);
+                    const double sum_avg = sum / in.n;
+                    if (h.in_aval && sum_avg < p.avalanche_speed_threshold) {
+                        ++h.aval_count;
+                        h.in_aval = false;
+                    } else if (sum_avg > p.avalanche_speed_threshold)
+                        h.in_aval = true;
+                }
             }
             D4_CUDA_OK(cudaMemcpyAsync(E->P.acc, acc.data(), sizeof(int) * E->count,
                                        cudaMemcpyHostToDevice, E->stream));

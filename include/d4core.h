@@ -244,7 +244,8 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
  * instance reproduces d4_run's arithmetic), then applies each instance's step
  * control as d4_run does (src/simulation.cpp:88-277; no log, sub-configuration
  * or write-out clipping).  An instance stays active until interrupt() holds
- * (time, strain or step-count limit, src/simulation.cpp:722-750). */
+ * (time, strain, step-count or avalanche limit, src/simulation.cpp:722-750;
+ * avalanches are counted as d4_run counts them). */
 int d4_ensemble_create(void **ens, int count, const int *n, const d4_params *p);
 int d4_ensemble_destroy(void *ens);
 const char *d4_ensemble_last_error(void *ens);

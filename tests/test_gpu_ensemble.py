@@ -100,3 +100,37 @@ def test_ensemble_time_limit_and_continuation(pkg, golden):
         assert np.array_equal(a.positions(k)[0], xs)
     a.close()
     b.close()
+
+
+def test_ensemble_avalanche_limit(pkg, golden):
+    """--avalanche-detection-limit 0: each instance stops when its first
+    avalanche (mean |v| above the threshold, then below it) ends, at the same
+    step as a single-system run with the same limit.  The threshold is twice
+    the mean |v| reached after 150 steps, so the relaxation's initial
+    avalanche ends within the step budget."""
+    cfg = configs(pkg, golden)[2:5]
+    base = dict(precision=1e-6, step_count_limited=True, step_count_limit=150)
+    means = []
+    for x, y in cfg:
+        sd = make_sd(pkg, **base)
+        sd.set_positions(x, y)
+        e = pkg.Engine(sd)
+        e.run()
+        xe, ye = e.positions()
+        v, _ = e.speeds(xe, ye, 0.0)
+        means.append(np.abs(v).mean())
+        e.close()
+    kw = dict(precision=1e-6, step_count_limited=True, step_count_limit=400,
+              count_avalanches=True, trigger_limit_for_avalanche_count=0,
+              avalanche_speed_threshold=2 * max(means))
+    ens = pkg.Ensemble(make_sd(pkg, **kw), cfg)
+    res = ens.run()
+    stopped_early = 0
+    for k, (x, y) in enumerate(cfg):
+        xs, rs = single(pkg, x, y, **kw)
+        assert (res[k].successful_steps, res[k].failed_steps) == (rs.successful_steps,
+                                                                  rs.failed_steps), k
+        assert np.array_equal(ens.positions(k)[0], xs), k
+        stopped_early += rs.successful_steps <= 400
+    assert stopped_early > 0
+    ens.close()
