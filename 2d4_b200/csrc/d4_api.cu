@@ -107,7 +107,7 @@ void free_all(Ctx *c) {
                     c->rowsub, c->rowsc,
                     c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
                     c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
-                    c->m_w1, c->m_resid};
+                    c->m_w1, c->m_resid, c->m_part, c->m_pp};
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
@@ -115,7 +115,7 @@ void free_all(Ctx *c) {
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
                   c->xw2_b, c->dx_b, B.A32, B.LU32, B.P0, B.Q, B.mask, B.bar, B.perm, B.piv,
-                  B.g, B.r, B.dx, B.c32, B.w1, B.resid, c->m_vacc_b};
+                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, c->m_vacc_b, c->m_pp_b};
     for (void *b : ob)
         if (b) cudaFree(b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -375,7 +375,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     }
     {
         ProfScope ps(c, D4_CAT_SPEEDS, sb);
-        d4::speeds32_with(c, c.m_vacc_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
+        d4::speeds32_with(c, c.m_vacc_b, c.m_pp_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE, sb);
@@ -720,6 +720,8 @@ int d4_create(void **out, int n, const d4_params *p) {
             for (double **v : mv) dalloc(v, (size_t)n);
             dalloc(&c->m_c32, (size_t)n);
             dalloc(&c->m_w1, (size_t)n);
+            dalloc(&c->m_part, (size_t)((n + 255) / 256) * n);
+            dalloc(&c->m_pp, (size_t)4 * ((n + 31) / 32) * n);
             dalloc(&c->m_resid, 16);
             D4_CUDA_OK(cudaMemset(c->m_resid, 0, sizeof(unsigned long long) * 16));
             D4_CUDA_OK(cudaMemset(c->A32, 0, sizeof(float) * nn));
@@ -791,12 +793,14 @@ int d4_create(void **out, int n, const d4_params *p) {
                 dalloc(&B.g, (size_t)n);
                 dalloc(&B.r, (size_t)n);
                 dalloc(&B.dx, (size_t)n);
+                dalloc(&B.part, (size_t)((n + 255) / 256) * n);
                 dalloc(&B.c32, (size_t)n);
                 dalloc(&B.w1, (size_t)n);
                 dalloc(&B.resid, 16);
                 D4_CUDA_OK(cudaMemset(B.resid, 0, sizeof(unsigned long long) * 16));
                 B.resid_count = &c->m_resid_count_b;
                 dalloc(&c->m_vacc_b, (size_t)n);
+                dalloc(&c->m_pp_b, (size_t)4 * ((n + 31) / 32) * n);
             }
         }
         d4::reset_tol64(*c);

@@ -46,6 +46,7 @@ struct Mix32Bufs {
     unsigned *mask = nullptr, *bar = nullptr;
     int *flags = nullptr, *perm = nullptr, *piv = nullptr;
     double *g = nullptr, *r = nullptr, *dx = nullptr;
+    double *part = nullptr;  // ceil(n / 256) x n: the residual product's column-chunk sums
     float *c32 = nullptr, *w1 = nullptr;
     unsigned long long *resid = nullptr;  // 8 pairs (max |r|, max |g|)
     int *resid_count = nullptr;           // host: next slot of resid
@@ -129,6 +130,8 @@ struct Ctx {
     double *m_vacc = nullptr, *m_subacc = nullptr, *m_g = nullptr, *m_r = nullptr,
            *m_dx = nullptr;
     float *m_c32 = nullptr, *m_w1 = nullptr;
+    double *m_part = nullptr;  // residual product's column-chunk sums (Mix32Bufs::part)
+    double *m_pp = nullptr, *m_pp_b = nullptr;  // pair-tile row partials, 4 x ceil(n/32) x n
     unsigned long long *m_resid = nullptr;  // 8 pairs (max |r|, max |g|) of recent solves
     int m_resid_count = 0;
     int ir_iters = 2;
@@ -250,9 +253,9 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
                          cudaStream_t st, int gmode, double hval, const double *s_end,
                          const double *s_init, const double *x_new, const double *x_old,
                          const double *base, double *out);
-// speeds32 with its own pair-sum scratch on `st`.
-void speeds32_with(Ctx &c, double *vacc, cudaStream_t st, const double *x, const double *y,
-                   double ext, double *v);
+// speeds32 with its own pair-sum scratch (row sums, tile partials) on `st`.
+void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const double *x,
+                   const double *y, double ext, double *v);
 int factor32(Ctx &c);
 int coop_grid_size32(int n);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,

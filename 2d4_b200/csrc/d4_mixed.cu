@@ -38,8 +38,10 @@ __device__ __forceinline__ void tile_of(int t, int T, int &ti, int &tj) {
 struct Pair32Args {
     int n;
     const double *x, *y;
-    double *vacc;    // FP64 sum of signed forces per dislocation (zeroed before)
-    double *subacc;  // FP64 sum of -J_ij per row (zeroed before; fused sweep)
+    double *vacc;    // FP64 sum of signed forces per dislocation (k_rowsum32)
+    double *subacc;  // FP64 sum of -J_ij per row (k_rowsum32; fused sweep)
+    double *part;    // 4 x T x n tile partials: [0] forces as row i, [1] as row j,
+                     // [2] -J as row i, [3] -J as row j (slot = the other tile index)
     float *A;        // raw J entries (fused sweep)
     double *tol;
     double min_prec_sq, h, cut_sq, cutoff, range_sq, one_per_cut_sq;
@@ -48,7 +50,9 @@ struct Pair32Args {
 
 // Unique pairs in 32x32 tiles (upper triangle); lanes walk i, threadIdx.y
 // steps j.  Row sums over the tile's j go through shared memory, column sums
-// over i through warp shuffles; one FP64 atomic per row and tile.
+// over i through warp shuffles; each tile stores one partial per row it
+// touches (no atomics), and k_rowsum32 adds them in tile order, so the sums
+// are the same on every run.
 template <bool kJac>
 __global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
     const int T = (a.n + 31) / 32;
@@ -108,8 +112,8 @@ __global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
             if (kJac) cj += __shfl_down_sync(0xffffffffu, cj, o);
         }
         if (tx == 0 && j < a.n) {
-            if (cf != 0) atomicAdd(a.vacc + j, cf);
-            if (kJac && cj != 0) atomicAdd(a.subacc + j, -cj);
+            a.part[((size_t)T + ti) * a.n + j] = cf;
+            if (kJac) a.part[((size_t)3 * T + ti) * a.n + j] = -cj;
         }
     }
     if (a.tol && i < a.n && row_min < a.min_prec_sq) tol_min(a.tol, i, row_min);
@@ -122,8 +126,8 @@ __global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
             sf += rs[k][tx];
             sj += rj[k][tx];
         }
-        if (sf != 0) atomicAdd(a.vacc + i, sf);
-        if (kJac && sj != 0) atomicAdd(a.subacc + i, -sj);
+        a.part[(size_t)tj * a.n + i] = sf;
+        if (kJac) a.part[((size_t)2 * T + tj) * a.n + i] = -sj;
     }
     if (kJac) {
         const int j = j0 + tx;
@@ -132,6 +136,26 @@ __global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
             if (ii < a.n && j < a.n && ii < j) a.A[(size_t)j + (size_t)ii * a.n] = sv[li][tx];
         }
     }
+}
+
+// Row r's partials in tile order: as row j of the tiles (tr, r/32), tr <= r/32,
+// then as row i of the tiles (r/32, tj), tj >= r/32.
+template <bool kJac>
+__global__ void k_rowsum32(int n, const double *part, double *vacc, double *subacc) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int T = (n + 31) / 32, R = r / 32;
+    double v = 0, w = 0;
+    for (int t = 0; t <= R; ++t) {
+        v += part[((size_t)T + t) * n + r];
+        if (kJac) w += part[((size_t)3 * T + t) * n + r];
+    }
+    for (int t = R; t < T; ++t) {
+        v += part[(size_t)t * n + r];
+        if (kJac) w += part[((size_t)2 * T + t) * n + r];
+    }
+    vacc[r] = v;
+    if (kJac) subacc[r] = w;
 }
 
 __global__ void k_speed_fin32(int n, const double *vacc, double ext, double *v) {
@@ -183,24 +207,34 @@ __global__ void k_ir_init(int n, trsv::GArgs ga, double *g, double *r, double *d
     dx[i] = 0;
 }
 
-// dx += c (float correction), r = g (reset before the matrix product).
-__global__ void k_ir_accum(int n, const float *c, const double *g, double *dx, double *r) {
+// dx += c (float correction); r is then recomputed from g by k_resid32.
+__global__ void k_ir_accum(int n, const float *c, double *dx) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     dx[i] += (double)c[i];
-    r[i] = g[i];
 }
 
-// r -= A32 dx over a chunk of columns per block (FP64 accumulation).
-__global__ void __launch_bounds__(256) k_gemv_sub32(int n, const float *__restrict__ A,
-                                                    const double *__restrict__ dx, double *r,
-                                                    int chunk) {
+// (A32 dx)_i over a chunk of columns per block (FP64 accumulation), into
+// part[chunk][i].
+__global__ void __launch_bounds__(256) k_gemv_part32(int n, const float *__restrict__ A,
+                                                     const double *__restrict__ dx, double *part,
+                                                     int chunk) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int c0 = blockIdx.y * chunk, c1 = min(n, c0 + chunk);
     if (i >= n) return;
     double s = 0;
     for (int c = c0; c < c1; ++c) s += (double)__ldg(A + (size_t)i + (size_t)c * n) * dx[c];
-    atomicAdd(r + i, -s);
+    part[(size_t)blockIdx.y * n + i] = s;
+}
+
+// r = g - A32 dx: the chunk sums subtracted in chunk order, so the residual,
+// and every correction computed from it, is the same on every run.
+__global__ void k_resid32(int n, const double *g, const double *part, int nch, double *r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = g[i];
+    for (int q = 0; q < nch; ++q) v = v - part[(size_t)q * n + i];
+    r[i] = v;
 }
 
 // max |r| and max |g| into out[0], out[1] (as ordered bits of non-negatives).
@@ -242,6 +276,7 @@ static Pair32Args pair32(Ctx &c, const double *x, const double *y) {
     a.y = y;
     a.vacc = c.m_vacc;
     a.subacc = c.m_subacc;
+    a.part = c.m_pp;
     a.A = c.A32;
     a.tol = c.use_dipole ? c.tol : nullptr;
     a.min_prec_sq = c.min_prec_sq;
@@ -259,29 +294,31 @@ static int pair_tiles(int n) {
     return T * (T + 1) / 2;
 }
 
-void speeds32_with(Ctx &c, double *vacc, cudaStream_t st, const double *x, const double *y,
-                   double ext, double *v) {
-    D4_CUDA_OK(cudaMemsetAsync(vacc, 0, sizeof(double) * c.n, st));
+void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const double *x,
+                   const double *y, double ext, double *v) {
     Pair32Args a = pair32(c, x, y);
     a.vacc = vacc;
+    a.part = part;
     k_pairs32<false><<<pair_tiles(c.n), dim3(32, 8), 0, st>>>(a);
     check_launch("k_pairs32<speeds>");
+    k_rowsum32<false><<<nb(c.n, 256), 256, 0, st>>>(c.n, part, vacc, nullptr);
+    check_launch("k_rowsum32<speeds>");
     k_speed_fin32<<<nb(c.n, 256), 256, 0, st>>>(c.n, vacc, ext, v);
     check_launch("k_speed_fin32");
 }
 
 void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v) {
-    speeds32_with(c, c.m_vacc, c.stream, x, y, ext, v);
+    speeds32_with(c, c.m_vacc, c.m_pp, c.stream, x, y, ext, v);
 }
 
 void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
                 double *v_a, double *v_b) {
-    D4_CUDA_OK(cudaMemsetAsync(c.m_vacc, 0, sizeof(double) * c.n, c.stream));
-    D4_CUDA_OK(cudaMemsetAsync(c.m_subacc, 0, sizeof(double) * c.n, c.stream));
     Pair32Args a = pair32(c, x, y);
     a.h = h;
     k_pairs32<true><<<pair_tiles(c.n), dim3(32, 8), 0, c.stream>>>(a);
     check_launch("k_pairs32<jacobian>");
+    k_rowsum32<true><<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_pp, c.m_vacc, c.m_subacc);
+    check_launch("k_rowsum32<jacobian>");
     k_jac_fin32<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_vacc, c.m_subacc, ext_a, ext_b,
                                                      v_a, v_b, c.dvec, c.fac, c.A32,
                                                      c.p.weight_function);
@@ -312,6 +349,7 @@ Mix32Bufs primary_mix32(Ctx &c) {
     B.g = c.m_g;
     B.r = c.m_r;
     B.dx = c.m_dx;
+    B.part = c.m_part;
     B.c32 = c.m_c32;
     B.w1 = c.m_w1;
     B.resid = c.m_resid;
@@ -398,10 +436,13 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
     const int chunk = 256;
     for (int it = 0; it < c.ir_iters; ++it) {
         solve32_once(c, B, st, B.r, B.c32);
-        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, B.c32, B.g, B.dx, B.r);
+        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, B.c32, B.dx);
         check_launch("k_ir_accum");
-        k_gemv_sub32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(n, B.A32, B.dx, B.r, chunk);
-        check_launch("k_gemv_sub32");
+        k_gemv_part32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(n, B.A32, B.dx, B.part,
+                                                                      chunk);
+        check_launch("k_gemv_part32");
+        k_resid32<<<nb(n, 256), 256, 0, st>>>(n, B.g, B.part, nb(n, chunk), B.r);
+        check_launch("k_resid32");
     }
     k_absmax2<<<64, 256, 0, st>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");
