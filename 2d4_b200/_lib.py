@@ -90,6 +90,7 @@ SIGNATURES = {
     "d4_lu_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 3),
     "d4_record_steps": (C.c_int, [_vp, C.c_int]),
     "d4_set_overlap": (C.c_int, [_vp, C.c_int]),
+    "d4_xpattern_df": (C.c_int, [C.c_int, _dp, _dp, C.POINTER(C.c_int), C.c_int, _dp]),
     "d4_recorded_count": (C.c_longlong, [_vp]),
     "d4_recorded_steps": (C.c_int, [_vp, C.c_longlong, _dp, _dp]),
     "d4_replay": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(Protocol), _dp, _dp, _dp]),

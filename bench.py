@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload c2|c1|c3-fp64] [--no-cpu-baseline] [--no-mixed]
-                    [--legs cutoff,tabulated,ensemble,adjoint|none]
+                    [--legs cutoff,tabulated,ensemble,adjoint,xpattern|none]
 
 A step is one ACCEPTED implicit step (stages I-IV of src/simulation.cpp:88-277;
 the failed attempts between accepted steps are part of its cost).  The metric is
@@ -31,7 +31,8 @@ all host cores) on the same workload, through Simulation::run, rank 0 only.
 At N=1 the line also carries bounded legs for the other configurations:
 mixed_vs_fp64 (N=4096 dense), cutoff (N=4096, Heaviside c = 0.1: FP64 dense,
 FP64 GMRES, mixed GMRES), tabulated (the N=1024 workload with the tabulated
-field), ensemble (512 instances of uneven N) and adjoint (N=2048, 200 steps).
+field), ensemble (512 instances of uneven N), adjoint (N=2048, 200 steps) and
+xpattern (direct-Fourier pattern analysis, N=4096 at resolution 1024).
 """
 import argparse
 import glob
@@ -330,6 +331,36 @@ def tabulated_leg(pkg, wl, steps=40):
             "max_position_diff_vs_analytic": d}
 
 
+def xpattern_leg(pkg, n=4096, res=1024, seed=1002, reps=3):
+    """Direct-Fourier pattern analysis (xpattern -m df) of one N=4096
+    configuration at resolution 1024 (K = 513: 263k k-points x 4096
+    dislocations): the GPU call end to end (host arrays in, host sums out,
+    its scratch allocated per call), best of `reps`, beside the numpy
+    restatement (complex GEMMs on all host cores) on the same input, and the
+    largest relative difference of the two (the CPU restatement is this leg's
+    CPU baseline and checker, never the product)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import xpattern_ref
+    xp = importlib.import_module("2d4_b200.xpattern")
+    x, y, _ = pkg.dconf.generate_internal(n, seed)
+    b = np.where(np.arange(n) < n // 2, 1.0, -1.0)
+    xp.direct_fourier(x, y, b, res)  # warm-up (module load, first allocation)
+    best = 1e9
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        got = xp.direct_fourier(x, y, b, res)
+        best = min(best, time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    ref = xpattern_ref.direct_fourier(x, y, b, res)
+    cpu = time.perf_counter() - t0
+    k = res // 2 + 1
+    return {"n": n, "resolution": res, "k_points": k * k, "gpu_seconds_e2e": best,
+            "dislocation_kpoints_per_s": n * k * k / best,
+            "cpu_baseline": {"seconds": cpu, "cores": os.cpu_count(), "kind": "port",
+                             "sample": "the same configuration, numpy complex GEMMs"},
+            "max_rel_diff_vs_cpu": float(np.abs(got - ref).max() / np.abs(ref).max())}
+
+
 def ensemble_leg(pkg, count=512, rounds=3, seed=2000):
     """The ensemble workload: `count` instances, N_k uniform over even values in
     [64, 2048] (seed 2000), positions seeds 3000 + k, tau_ext = 1e-3 t, time
@@ -436,7 +467,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the N=4096 mixed vs FP64 leg")
-    ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint",
+    ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint,xpattern",
                     help="extra single-GPU legs (comma list, or 'none')")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -552,7 +583,8 @@ def main():
     for name, fn in (("cutoff", lambda: cutoff_leg(pkg)),
                      ("tabulated", lambda: tabulated_leg(pkg, wl)),
                      ("ensemble", lambda: ensemble_leg(pkg)),
-                     ("adjoint", lambda: adjoint_leg(pkg))):
+                     ("adjoint", lambda: adjoint_leg(pkg)),
+                     ("xpattern", lambda: xpattern_leg(pkg))):
         if ws == 1 and name in legs:
             try:
                 line[name] = fn()

@@ -258,6 +258,18 @@ int d4_ensemble_get_positions(void *ens, int k, double *x, double *y);
  * every entry, device_seconds = the CUDA-event span of this call. */
 int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res);
 
+/* Direct-Fourier pattern analysis of one configuration (the reference's
+ * xpattern tool, method df, xpattern/xpattern.cpp:393-423).  With K = res/2+1
+ * and F_m(kx, ky) = sum_i w_m(b_i) exp(-2 pi i (kx x_i + ky y_i)) for the four
+ * densities m = rho_t (w = 1), kappa (w = b), rho_p (b = +1) and rho_n
+ * (b = -1), adds sum_ky |F_m(kx, ky)|^2 (ky ascending) to acc[m*K + kx],
+ * kx = 0..K-1, so that repeated calls sum over configurations as the tool
+ * does over its input files.  x, y, b: host arrays of n entries; acc: host,
+ * 4*K entries, read and updated.  FP64 throughout; 2 <= res <= 65536.  Uses
+ * the current device and allocates its scratch (two n x K tables and 4 K^2
+ * doubles) for the call. */
+int d4_xpattern_df(int n, const double *x, const double *y, const int *b, int res, double *acc);
+
 /* Schedule of an attempt (dense plain and mixed forms): enable = 1 (the
  * default) runs stage I, the big step, on a second stream concurrently with
  * stages II and III; 0 runs the stages one after the other on the context's
