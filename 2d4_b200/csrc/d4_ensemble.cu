@@ -350,13 +350,24 @@ __global__ void __launch_bounds__(kLuT) k_ens_lu(Pools P, const Inst *ins, const
                     for (int q = 0; q < 4; ++q) lv[q] = sL[tr + 16 * q][c];
 #pragma unroll
                     for (int w = 0; w < 4; ++w) uv[w] = sU[c][tc + 16 * w];
+                    // the oracle skips an update whose u_kj is 0; when no u of
+                    // this warp's columns is 0 (the dense case) the plain
+                    // product-difference is the same and needs no select
+                    const bool nz = uv[0] != 0.0 && uv[1] != 0.0 && uv[2] != 0.0 && uv[3] != 0.0;
+                    if (__all_sync(0xffffffffu, nz)) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
+                        for (int q = 0; q < 4; ++q)
 #pragma unroll
-                        for (int w = 0; w < 4; ++w) {
-                            const double nv = acc[q][w] - lv[q] * uv[w];
-                            acc[q][w] = uv[w] != 0.0 ? nv : acc[q][w];
-                        }
+                            for (int w = 0; w < 4; ++w) acc[q][w] = acc[q][w] - lv[q] * uv[w];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+#pragma unroll
+                            for (int w = 0; w < 4; ++w) {
+                                const double nv = acc[q][w] - lv[q] * uv[w];
+                                acc[q][w] = uv[w] != 0.0 ? nv : acc[q][w];
+                            }
+                    }
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
