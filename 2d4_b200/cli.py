@@ -31,7 +31,7 @@ import os
 import sys
 import time
 
-from . import _lib, dconf
+from . import _lib
 from .simulation import (CyclicLoadProtocol, FixedRateProtocol, IncreasingCyclicLoadProtocol,
                          SimulationData, StressProtocol)
 
