@@ -144,3 +144,22 @@ def test_simulation_data_params(pkg, tmp_path):
     assert c.position_precision == 1e-8 and c.step_count_limit == 999
     assert c.protocol.kind == 1 and c.protocol.tau0 == 0.05
     assert c.time_limit < 0 and c.max_stepsize < 0
+
+
+def test_new_entry_points_reject_bad_arguments(pkg):
+    """The overlap switch, the LU counters and the pattern analysis check
+    their arguments before any device work (status -1, D4_ERR_ARG)."""
+    lib = pkg._lib.load()
+    v = C.c_longlong()
+    assert lib.d4_set_overlap(None, 1) == -1
+    assert lib.d4_lu_stats(None, C.byref(v), C.byref(v), C.byref(v)) == -1
+    x = np.zeros(4)
+    b = np.array([1, 1, -1, -1], dtype=np.int32)
+    acc = np.zeros(4 * 9)
+    ip = b.ctypes.data_as(C.POINTER(C.c_int))
+    dp = pkg._lib.ptr
+    assert lib.d4_xpattern_df(-1, dp(x), dp(x), ip, 16, dp(acc)) == -1   # negative n
+    assert lib.d4_xpattern_df(4, dp(x), dp(x), ip, 1, dp(acc)) == -1     # resolution < 2
+    assert lib.d4_xpattern_df(4, None, dp(x), ip, 16, dp(acc)) == -1     # missing input
+    assert lib.d4_xpattern_df(4, dp(x), dp(x), ip, 16, None) == -1       # missing sums
+    assert lib.d4_xpattern_df(4, dp(x), dp(x), ip, 70000, dp(acc)) == -1  # beyond the maximum
