@@ -40,15 +40,43 @@ def test_oracle_vectorised_equals_loops():
     assert np.allclose(a[0] + a[1], 2 * (a[2] + a[3]), rtol=1e-12)
 
 
-def test_cli_rejects_other_methods(tmp_path):
-    assert xp.main(["-i", str(tmp_path / "a.dconf"), "-m", "bc"], io.StringIO()) == 255
+def test_cli_options_and_checks(tmp_path):
+    """The tool's option names, defaults and input checks (status, message)."""
+    d = tmp_path / "a.dconf"
+    d.write_text("0.1 0.2 1\n-0.1 0.3 -1\n")
+    def run(argv):
+        out, err = io.StringIO(), io.StringIO()
+        return xp.main(argv, out, err), out.getvalue() + err.getvalue()
+    st, msg = run([])
+    assert st == 255 and "input-fname is missing!" in msg
+    st, msg = run(["-i", str(d), "--no-such-option"])
+    assert st == 255 and "unrecognized" in msg
+    st, msg = run(["-i", str(d)])  # the tool's default method is bc, not built here
+    assert st == 255 and "bc is not built here" in msg
+    st, msg = run(["-i", str(d), "-m", "xx"])
+    assert st == 255 and "xx is unknown" in msg
+    st, msg = run(["-i", str(d), "-m", "df", "-r", "1"])
+    assert st == 255 and "resulution is smaller than 2" in msg
+    st, msg = run(["-i", str(d), "-m", "df", "--create-maps"])
+    assert st == 255
+    st, msg = run(["-i", str(tmp_path / "a.txt"), "-m", "df"])
+    assert st == 1 and "is not a valid input filename" in msg
+    ini = tmp_path / "l.ini"
+    ini.write_text("a.dconf b.txt\n")
+    st, msg = run(["-i", str(ini), "-m", "df"])
+    assert st == 2 and "contains invalid dislocation configuration filename b.txt" in msg
+    ini.write_text("\n")
+    st, msg = run(["-i", str(ini), "-m", "df"])
+    assert st == 1 and "Not enough input files" in msg
+    st, msg = run(["-i", str(tmp_path / "none.ini"), "-m", "df"])
+    assert st == 0 and "couldn't open" in msg
 
 
 def test_input_list(tmp_path):
     lst = tmp_path / "files.ini"
-    lst.write_text("a.dconf\n\nb.dconf\n")
-    assert xp.input_files(str(lst)) == ["a.dconf", "b.dconf"]
-    assert xp.input_files("c.dconf") == ["c.dconf"]
+    lst.write_text("a.dconf\n\nb.dconf c.dconf\n")
+    assert xp.input_files(str(lst), io.StringIO()) == ["a.dconf", "b.dconf", "c.dconf"]
+    assert xp.input_files("c.dconf", io.StringIO()) == ["c.dconf"]
 
 
 @pytest.mark.gpu
@@ -102,8 +130,8 @@ def test_xpattern_cli_files(pkg, tmp_path):
     lst = tmp_path / "list.ini"
     lst.write_text("\n".join(paths) + "\n")
     prefix = str(tmp_path / "out_")
-    assert xp.main(["-i", str(lst), "-r", "64", "-o", prefix, "--digits", "17"],
-                   io.StringIO()) == 0
+    assert xp.main(["-c", "-i", str(lst), "-m", "df", "-r", "64", "-o", prefix, "-s", "4",
+                    "-d", "1", "--digits", "17"], io.StringIO()) == 0
     ref = sum(xpattern_ref.direct_fourier(*pkg.dconf.read(p), 64) for p in paths)
     for m, name in enumerate(xp.NAMES):
         lines = open("%sdf_r64_%s_k.txt" % (prefix, name)).read().splitlines()
