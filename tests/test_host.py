@@ -163,3 +163,29 @@ def test_new_entry_points_reject_bad_arguments(pkg):
     assert lib.d4_xpattern_df(4, None, dp(x), ip, 16, dp(acc)) == -1     # missing input
     assert lib.d4_xpattern_df(4, dp(x), dp(x), ip, 16, None) == -1       # missing sums
     assert lib.d4_xpattern_df(4, dp(x), dp(x), ip, 70000, dp(acc)) == -1  # beyond the maximum
+
+
+def test_size_limits_rejected_before_device_work(pkg):
+    """N outside 2..8192 or odd (the largest system whose substitution vector
+    fits one CTA's shared memory; balanced Burgers vectors need even N), and
+    ensembles with such an instance, a non-FP64 form or the GMRES solver, are
+    refused with D4_ERR_ARG before any device call."""
+    lib = pkg._lib.load()
+    p = pkg._lib.Params()
+    ctx = C.c_void_p()
+    for n in (0, -2, 1, 8194, 1 << 20):
+        lib.d4_default_params(C.byref(p))
+        assert lib.d4_create(C.byref(ctx), n, C.byref(p)) == -1, n
+    ens = C.c_void_p()
+    for sizes in ([64, 8194], [64, 63], [0], [2, -4]):
+        lib.d4_default_params(C.byref(p))
+        arr = (C.c_int * len(sizes))(*sizes)
+        assert lib.d4_ensemble_create(C.byref(ens), len(sizes), arr, C.byref(p)) == -1, sizes
+    arr = (C.c_int * 2)(64, 128)
+    assert lib.d4_ensemble_create(C.byref(ens), 0, arr, C.byref(p)) == -1
+    for kw in (dict(precision=pkg._lib.D4_PREC_MIXED), dict(field=pkg._lib.D4_FIELD_TABULATED),
+               dict(solver=pkg._lib.D4_SOLVER_GMRES), dict(weight_function=b"x")):
+        lib.d4_default_params(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        assert lib.d4_ensemble_create(C.byref(ens), 2, arr, C.byref(p)) == -1, kw
