@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libd4core.so")
 
 D4_OK, D4_WARN_SINGULAR = 0, 1
+D4_ERR_ARG, D4_ERR_CUDA, D4_ERR_NOMEM, D4_ERR_STATE, D4_ERR_IO = -1, -2, -3, -4, -5
 D4_ERR = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "bad state",
           -5: "I/O error"}
 D4_PREC_FP64, D4_PREC_MIXED = 0, 1
@@ -86,8 +87,15 @@ SIGNATURES = {
     "d4_profile": (C.c_int, [_vp, C.c_int]),
     "d4_profile_read": (C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)]),
     "d4_kernel_launches": (C.c_longlong, []),
+    "d4_device_allocations": (C.c_longlong, []),
+    "d4_check_positions": (C.c_int, [C.c_int, _dp, _dp]),
+    "d4_wait_selftest": (C.c_int, [_vp, C.c_int]),
     "d4_solver_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 4),
     "d4_lu_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 3),
+    "d4_mixed_stats": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), _dp]),
+    "d4_set_block_lu": (C.c_int, [_vp, C.c_int]),
+    "d4_pair_tile_threads": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "d4_ensemble_pair_tile_threads": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "d4_record_steps": (C.c_int, [_vp, C.c_int]),
     "d4_set_overlap": (C.c_int, [_vp, C.c_int]),
     "d4_xpattern_df": (C.c_int, [C.c_int, _dp, _dp, C.POINTER(C.c_int), C.c_int, _dp]),

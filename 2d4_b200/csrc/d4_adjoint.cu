@@ -354,13 +354,13 @@ struct Work {
     std::vector<void *> bufs;
     double *alloc(size_t count) {
         void *p = nullptr;
-        D4_CUDA_OK(cudaMalloc(&p, sizeof(double) * (count ? count : 1)));
+        D4_CUDA_OK(d4::dmalloc(&p, sizeof(double) * (count ? count : 1)));
         bufs.push_back(p);
         return static_cast<double *>(p);
     }
     int *ialloc(size_t count) {
         void *p = nullptr;
-        D4_CUDA_OK(cudaMalloc(&p, sizeof(int) * (count ? count : 1)));
+        D4_CUDA_OK(d4::dmalloc(&p, sizeof(int) * (count ? count : 1)));
         bufs.push_back(p);
         return static_cast<int *>(p);
     }

@@ -11,6 +11,7 @@
 #include <fstream>
 #include <iomanip>
 #include <algorithm>
+#include <chrono>
 #include <new>
 #include <sstream>
 #include <string>
@@ -23,6 +24,7 @@ using d4::CudaError;
 
 namespace d4 {
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_allocs{0};
 
 int prof_begin(Ctx &c, int cat, cudaStream_t st) {
     if (!c.prof.on) return -1;
@@ -79,6 +81,14 @@ namespace {
 
 inline double ext_stress(const d4_protocol &p, double t) { return d4::ext_stress_host(p, t); }
 
+// get_wall_time, src/sim_utils.cpp:22-33: seconds of the wall clock, at the
+// reference's millisecond resolution.
+double wall_time() {
+    const auto ms = std::chrono::time_point_cast<std::chrono::milliseconds>(
+        std::chrono::high_resolution_clock::now());
+    return static_cast<double>(ms.time_since_epoch().count()) / 1000.;
+}
+
 // SimulationData::getNextWriteOutTime, src/simulation_data.cpp:231-246.
 double next_write_out(const d4_params &p, double sim_time) {
     if (p.sub_config_times == 0) return INFINITY;
@@ -96,7 +106,7 @@ double next_write_out(const d4_params &p, double sim_time) {
 
 template <typename T>
 void dalloc(T **p, size_t count) {
-    D4_CUDA_OK(cudaMalloc((void **)p, sizeof(T) * (count > 0 ? count : 1)));
+    D4_CUDA_OK(d4::dmalloc((void **)p, sizeof(T) * (count > 0 ? count : 1)));
 }
 
 void free_all(Ctx *c) {
@@ -111,6 +121,9 @@ void free_all(Ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
+    d4::blu_free(c->blu);
+    d4::blu_free(c->m32b.blu);
+    if (c->blu_tasks) cudaFree(c->blu_tasks);
     const d4::Mix32Bufs &B = c->m32b;
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
@@ -463,7 +476,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
 }
 
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
-int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
+static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
     if (c.overlap) {
         int singular = 0;
         double refine = 0;
@@ -584,6 +597,31 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     return D4_OK;
 }
 
+// One attempted step.  In the mixed form the factorisations are block LUs
+// without row interchanges (d4_blu32.cu); when one of them met a zero or
+// non-finite pivot in a diagonal tile, or a refined solve kept a residual
+// above kRefineLimit, the attempt is redone with the pivoted cooperative LU,
+// so its result is that of the exact-pivoting path.
+int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
+    if (c.p.precision != D4_PREC_MIXED || !c.m_fast) return attempt_once(c, t0, h, res);
+    const long long before = c.m_blocklu;
+    attempt_once(c, t0, h, res);
+    if (c.m_blocklu == before) return D4_OK;  // no dense factorisation ran (GMRES)
+    const double rr = res->refine_residual;
+    if (!(rr <= c.m_worst_refine)) c.m_worst_refine = rr;
+    if (!res->singular && rr <= d4::kRefineLimit) return D4_OK;
+    ++c.m_fallbacks;
+    c.m_fast = 0;
+    try {
+        attempt_once(c, t0, h, res);
+    } catch (...) {
+        c.m_fast = 1;
+        throw;
+    }
+    c.m_fast = 1;
+    return D4_OK;
+}
+
 // Stress sweep of the context's form (FP64 buffers exist only in the FP64 form).
 void sweep_speeds(Ctx &c, const double *x, const double *y, double ext, double *v) {
     if (c.p.precision == D4_PREC_MIXED)
@@ -638,6 +676,16 @@ void write_config(Ctx &c, const std::string &path, const unsigned *order) {
 }  // namespace
 
 extern "C" {
+
+int d4_check_positions(int n, const double *x, const double *y) {
+    if (n < 0 || (n > 0 && (!x || !y))) return -2;
+    for (int i = 0; i < n; ++i) {
+        // finite and inside the periodic cell, where normalize
+        // (src/sim_utils.cpp:6-13) keeps every position
+        if (!(x[i] >= -0.5 && x[i] < 0.5 && y[i] >= -0.5 && y[i] < 0.5)) return i;
+    }
+    return -1;
+}
 
 void d4_default_params(d4_params *p) {
     std::memset(p, 0, sizeof(*p));
@@ -727,6 +775,11 @@ int d4_create(void **out, int n, const d4_params *p) {
             D4_CUDA_OK(cudaMemset(c->A32, 0, sizeof(float) * nn));
             c->lu32_grid = d4::coop_grid_size32(n);
             if (c->lu32_grid < 0) throw d4::StateError("n too large for the cooperative LU");
+            const std::vector<int> sched = d4::blu_schedule(n);
+            dalloc(&c->blu_tasks, sched.size());
+            D4_CUDA_OK(cudaMemcpy(c->blu_tasks, sched.data(), sizeof(int) * sched.size(),
+                                  cudaMemcpyHostToDevice));
+            d4::blu_alloc(c->blu, n, c->blu_tasks, &c->blu_state);
         }
         dalloc(&c->piv, (size_t)n);
         dalloc(&c->perm, (size_t)n);
@@ -799,6 +852,8 @@ int d4_create(void **out, int n, const d4_params *p) {
                 dalloc(&B.resid, 16);
                 D4_CUDA_OK(cudaMemset(B.resid, 0, sizeof(unsigned long long) * 16));
                 B.resid_count = &c->m_resid_count_b;
+                B.blk = &c->m_blk_b;
+                d4::blu_alloc(B.blu, n, c->blu_tasks, &c->blu_state_b);
                 dalloc(&c->m_vacc_b, (size_t)n);
                 dalloc(&c->m_pp_b, (size_t)4 * ((n + 31) / 32) * n);
             }
@@ -835,6 +890,11 @@ const char *d4_last_error(void *ctx) {
 int d4_set_positions(void *ctx, const double *x, const double *y) {
     Ctx *c = (Ctx *)ctx;
     if (!c || !x || !y) return D4_ERR_ARG;
+    const int bad = d4_check_positions(c->n, x, y);
+    if (bad >= 0)
+        return fail(c, D4_ERR_ARG,
+                    "d4_set_positions: dislocation " + std::to_string(bad) +
+                        " is not finite or outside the cell [-0.5, 0.5)^2");
     D4_GUARD_BEGIN
     upload(*c, c->x0, x);
     upload(*c, c->y, y);
@@ -932,10 +992,19 @@ int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *
 int d4_set_matrix(void *ctx, const double *a_colmajor) {
     Ctx *c = (Ctx *)ctx;
     if (!c || !a_colmajor) return D4_ERR_ARG;
-    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_set_matrix: FP64 form only");
     D4_GUARD_BEGIN
-    D4_CUDA_OK(cudaMemcpyAsync(c->A, a_colmajor, sizeof(double) * (size_t)c->n * c->n,
-                               cudaMemcpyHostToDevice, c->stream));
+    const size_t nn = (size_t)c->n * c->n;
+    if (c->p.precision == D4_PREC_MIXED) {
+        // the mixed form's matrix is FP32 (rounded to nearest)
+        std::vector<float> a32(nn);
+        for (size_t k = 0; k < nn; ++k) a32[k] = (float)a_colmajor[k];
+        D4_CUDA_OK(cudaMemcpyAsync(c->A32, a32.data(), sizeof(float) * nn,
+                                   cudaMemcpyHostToDevice, c->stream));
+        sync(*c);
+        return D4_OK;
+    }
+    D4_CUDA_OK(cudaMemcpyAsync(c->A, a_colmajor, sizeof(double) * nn, cudaMemcpyHostToDevice,
+                               c->stream));
     sync(*c);
     return D4_OK;
     D4_GUARD_END(c)
@@ -945,7 +1014,7 @@ int d4_factor(void *ctx) {
     Ctx *c = (Ctx *)ctx;
     if (!c) return D4_ERR_ARG;
     D4_GUARD_BEGIN
-    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_factor: FP64 form only");
+    if (c->p.precision == D4_PREC_MIXED) return d4::factor32(*c);
     return d4::factor64(*c);
     D4_GUARD_END(c)
 }
@@ -953,9 +1022,17 @@ int d4_factor(void *ctx) {
 int d4_solve(void *ctx, const double *g, double *dx) {
     Ctx *c = (Ctx *)ctx;
     if (!c || !g || !dx) return D4_ERR_ARG;
-    if (c->p.precision == D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_solve: FP64 form only");
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, g);
+    if (c->p.precision == D4_PREC_MIXED) {
+        d4::solve_plain32(*c, c->xs_tmp);
+        download(*c, dx, c->dx);
+        read_async_errors(*c);
+        int fl[d4::kFlagCount];
+        D4_CUDA_OK(cudaMemcpy(fl, c->flags, sizeof(fl), cudaMemcpyDeviceToHost));
+        if (fl[d4::kFlagBarrierTimeout]) throw d4::StateError("block solve wait timed out");
+        return c->factor_singular ? D4_WARN_SINGULAR : D4_OK;
+    }
     d4::solve_plain64(*c, c->xs_tmp);
     download(*c, dx, c->dx);
     sync(*c);
@@ -989,7 +1066,7 @@ int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, doub
     if (!c || count < 0 || !dx || !dy || !xy || !xyd) return D4_ERR_ARG;
     D4_GUARD_BEGIN
     double *d = nullptr;
-    D4_CUDA_OK(cudaMalloc((void **)&d, sizeof(double) * 4 * (size_t)(count > 0 ? count : 1)));
+    D4_CUDA_OK(d4::dmalloc((void **)&d, sizeof(double) * 4 * (size_t)(count > 0 ? count : 1)));
     const size_t b = sizeof(double) * (size_t)count;
     cudaMemcpyAsync(d, dx, b, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(d + count, dy, b, cudaMemcpyHostToDevice, c->stream);
@@ -1028,6 +1105,15 @@ static int run_loop(Ctx *c, const d4_run_io *io, std::ofstream *log, long long t
         const double h = c->step_size;
         d4_attempt_result ar;
         attempt(*c, c->sim_time, h, &ar);
+        if (!std::isfinite(ar.ratio)) {
+            // a NaN ratio fails every attempt while getNewStepSize keeps
+            // doubling h (min(2, NaN^(-1/6)) is 2): stop with an error instead,
+            // as the reference's DEBUG_VERSION checks stop on non-finite state
+            // (src/simulation.cpp:754-948)
+            c->err_detail = "non-finite error ratio at t = " + std::to_string(c->sim_time) +
+                            ", h = " + std::to_string(h) + ": positions or speeds are not finite";
+            throw d4::StateError(c->err_detail.c_str());
+        }
         ++rs.attempts;
         rs.pivoted += ar.pivoted;
         rs.singular += ar.singular;
@@ -1071,12 +1157,17 @@ static int run_loop(Ctx *c, const d4_run_io *io, std::ofstream *log, long long t
                     *log << op << "\t";
                 } else
                     *log << "-\t";
-                *log << ext_stress(p.protocol, c->sim_time) << "\t" << 0 << "\t";
+                // columns 10 and 14: wall time since the previous log line and
+                // since the start of the run (src/simulation.cpp:197,206)
+                *log << ext_stress(p.protocol, c->sim_time) << "\t" << wall_time() - rs.wall_last
+                     << "\t";
                 if (p.calculate_strain)
                     *log << rs.strain << "\t";
                 else
                     *log << "-\t";
-                *log << vsq_end << "\t" << rs.energy << "\t" << 0 << "\t" << h << "\n";
+                *log << vsq_end << "\t" << rs.energy << "\t" << wall_time() - rs.wall_start
+                     << "\t" << h << "\n";
+                rs.wall_last = wall_time();
             }
             if (p.avalanche_limit >= 0) {
                 if (rs.in_aval && sum_avg < p.avalanche_speed_threshold) {
@@ -1155,7 +1246,9 @@ int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
         if (!log) return fail(c, D4_ERR_IO, std::string("cannot open log ") + io->log_path);
         log << std::scientific << std::setprecision(16);
     }
+    if (c->p.precision == D4_PREC_FP64) d4::autotune_pairs(*c);
     start_state(c);
+    c->rs.wall_start = c->rs.wall_last = wall_time();
     const d4::RunState before = c->rs;
     D4_CUDA_OK(cudaEventRecord(c->ev0, c->stream));
     // src/simulation.cpp:46: initial speeds (also seeds the tolerances)
@@ -1188,6 +1281,7 @@ int d4_advance(void *ctx, long long accepted_steps, d4_run_result *res) {
     Ctx *c = (Ctx *)ctx;
     if (!c || accepted_steps < 0) return D4_ERR_ARG;
     D4_GUARD_BEGIN
+    if (c->p.precision == D4_PREC_FP64) d4::autotune_pairs(*c);
     if (!c->rs.started) {
         start_state(c);
         // the first attempt's tolerances include the initial sweep of run()
@@ -1258,6 +1352,31 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
     return D4_OK;
 }
 
+int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
+                   double *worst_refined) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !block_factorizations || !fallbacks || !worst_refined) return D4_ERR_ARG;
+    *block_factorizations = c->m_blocklu;
+    *fallbacks = c->m_fallbacks;
+    *worst_refined = c->m_worst_refine;
+    return D4_OK;
+}
+
+int d4_pair_tile_threads(void *ctx, int *threads_y) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !threads_y) return D4_ERR_ARG;
+    *threads_y = c->pair_tuned ? c->pair_ty : 0;
+    return D4_OK;
+}
+
+int d4_set_block_lu(void *ctx, int enable) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c) return D4_ERR_ARG;
+    if (c->p.precision != D4_PREC_MIXED) return fail(c, D4_ERR_ARG, "d4_set_block_lu: mixed form only");
+    c->m_fast = enable ? 1 : 0;
+    return D4_OK;
+}
+
 int d4_record_steps(void *ctx, int enable) {
     Ctx *c = (Ctx *)ctx;
     if (!c) return D4_ERR_ARG;
@@ -1286,5 +1405,20 @@ int d4_recorded_steps(void *ctx, long long count, double *t0s, double *hs) {
 }
 
 long long d4_kernel_launches(void) { return d4::g_launches.load(); }
+
+long long d4_device_allocations(void) { return d4::g_allocs.load(); }
+
+int d4_wait_selftest(void *ctx, int which) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || which < 0 || which > 1) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    D4_CUDA_OK(cudaSetDevice(c->p.device));
+    const int st = d4::wait_selftest(which);
+    if (st == D4_ERR_STATE)
+        return fail(c, st, which == 0 ? "grid barrier wait gave up (self-test)"
+                                      : "tile flag wait gave up (self-test)");
+    return st;
+    D4_GUARD_END(c)
+}
 
 }  // extern "C"

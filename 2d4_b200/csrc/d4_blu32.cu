@@ -1,0 +1,703 @@
+// d4_blu32.cu: the mixed form's factorisation and triangular solves.
+//
+// Block LU of the FP32 Jacobian in 128 x 128 tiles without row interchanges
+// between tiles:
+//     A = L U,  L block unit-lower, U block upper with full diagonal blocks,
+//     S_ij = A_ij - sum_{k < min(i,j)} L_ik U_kj
+//     i == j:  D_j = S_jj^-1   (Gauss-Jordan of the tile, kept for the solves)
+//     i >  j:  L_ij = S_ij D_j
+//     i <  j:  U_ij = S_ij
+// so the solve of A x = b is  y_i = b_i - sum_{k<i} L_ik y_k,
+// x_i = D_i (y_i - sum_{j>i} U_ij x_j).  Every product runs on the tensor
+// cores (tcgen05.mma kind::tf32, FP32 accumulators in TMEM) as hi*hi + hi*lo
+// + lo*hi of the operands split into TF32 hi and lo parts, which keeps the
+// factors close to FP32 accuracy; the FP64 refinement of each solve (against
+// the FP32 matrix, d4_mixed.cu) removes the rest.  The mixed form has no
+// bit-parity duty, so the exact-order partial pivoting of the FP64 form is
+// replaced by this pivot-free block form; a tile whose Gauss-Jordan meets a
+// zero or non-finite pivot sets kFlagSingular, and the caller redoes the
+// attempt with the pivoted cooperative LU (d4_lu_coop.cuh) — as it does when
+// a refined residual stays large.
+//
+// Scheduling.  One persistent launch; each CTA takes the next tile from a
+// ticket counter in the order ring m = 0, 1, ... (ring m: the tiles with
+// min(i, j) = m, diagonal first, then the pairs (m+d, m), (m, m+d) by
+// increasing d).  A tile depends only on tiles earlier in that order, which
+// CTAs that are already running hold, so the launch needs no co-residency.
+// Finished tiles publish an epoch flag (release); a CTA waits for its
+// operands' flags (acquire, bounded) before copying them.
+//
+// Each finished tile is stored twice: plainly into LU (column-major n x n,
+// read by the solves) and as tensor-core operands into its slot of `op`: the
+// TF32 hi and lo parts (64 KiB each) in the canonical K-major layout without
+// swizzle (8-row x 16-byte core matrices; 32-wide K chunks of 16 KiB), L_ik
+// with rows as M, U_kj and D_j with columns as N.  A CTA streams the operand
+// chunks of its accumulation with untiled bulk copies (cp.async.bulk, this
+// GPU's memory only, no multicast) into a three-stage shared-memory ring;
+// thread 0 issues the copies and the MMAs (one elected thread per CTA) and
+// tcgen05.commit frees each stage.
+#include <cstdint>
+
+#include "d4_bulk.cuh"
+#include "d4_internal.h"
+#include "d4_lu_coop.cuh"
+
+namespace d4 {
+namespace blu {
+
+constexpr int kB = 128;
+constexpr int kThreads = 256;
+constexpr int kStages = 3;
+constexpr uint32_t kStageBytes = 65536;  // A hi, A lo, B hi, B lo chunks of 16 KiB
+constexpr uint32_t kChunkBytes = 16384;
+constexpr size_t kPartBytes = 65536;     // one packed 128 x 128 FP32 tile
+constexpr size_t kSlotBytes = 2 * kPartBytes;
+constexpr int kSp = 129;                 // row stride (floats) of the plain tile in shared memory
+constexpr size_t kRingBytes = (size_t)kStages * kStageBytes;
+constexpr size_t kBarOff = kRingBytes;   // barriers: full[3], empty[3], acc
+constexpr size_t kSmemBytes = kRingBytes + 1024;
+constexpr long long kSpin = 1ll << 24;   // flag polls (each >= 64 ns): > 1 s
+static_assert((size_t)kB * kSp * 4 + 4096 <= kRingBytes, "plain tile and GJ buffers fit the ring");
+
+struct Args {
+    int n, T;
+    const float *A;         // n x n column-major
+    float *LU;              // n x n column-major: L_ij (i > j), U_ij (i < j), D_j (diagonal)
+    unsigned char *op;      // T*T slots of kSlotBytes
+    const int *tasks;       // T*T: (i << 16) | j in schedule order
+    int *ticket;            // ticket counter (zeroed before the launch)
+    int *ready;             // T*T tile flags (== epoch: done)
+    int epoch;
+    int *flags;             // kFlagSingular, kFlagBarrierTimeout
+};
+
+__device__ __forceinline__ uint32_t poff(int R, int K) {
+    return (uint32_t)((K >> 5) * 16384 + ((K & 31) >> 2) * 2048 + (R >> 3) * 128 + (R & 7) * 16 +
+                      (K & 3) * 4);
+}
+
+__device__ __forceinline__ int ld_acq(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_rel(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void fence_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait for flag == epoch; false (and kFlagBarrierTimeout) if it gave up
+// or another CTA already gave up.
+__device__ bool wait_flag(const int *f, int epoch, int *flags) {
+    long long spins = 0;
+    while (ld_acq(f) != epoch) {
+        __nanosleep(64);
+        if ((++spins & 255) == 0 &&
+            (spins > kSpin || ld_acq(&flags[kFlagBarrierTimeout]))) {
+            atomicOr(&flags[kFlagBarrierTimeout], 1);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void gave_up(int *flags) { atomicOr(&flags[kFlagBarrierTimeout], 1); }
+
+// The 12 MMAs of one 32-wide K chunk held in stage `sb` (shared address):
+// A hi/lo at +0/+16K, B hi/lo at +32K/+48K; hi*hi + hi*lo + lo*hi.
+__device__ __forceinline__ void mma_chunk(uint32_t tmem_d, uint32_t sb, bool first) {
+    using namespace coop::tc;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const uint32_t o = u * 4096;
+        mma(tmem_d, desc(sb + o), desc(sb + 32768 + o), (first && u == 0) ? 0u : 1u);
+        mma(tmem_d, desc(sb + o), desc(sb + 49152 + o), 1u);
+        mma(tmem_d, desc(sb + 16384 + o), desc(sb + 32768 + o), 1u);
+    }
+}
+
+__device__ __forceinline__ void ld64(uint32_t taddr, float (&v)[64]) {
+    float a[32], b[32];
+    coop::tc::ld32(taddr, a);
+    coop::tc::ld32(taddr + 32, b);
+#pragma unroll
+    for (int t = 0; t < 32; ++t) {
+        v[t] = a[t];
+        v[32 + t] = b[t];
+    }
+}
+
+// A tile F (plain, row-major, stride kSp, in shared memory) of tile position
+// (ti, tj) to LU (real entries) and to its operand slot: A format (rows as M)
+// when !bfmt, else B format (columns as N).
+__device__ void store_tile(const Args &a, const float *Sp, int ti, int tj, bool bfmt,
+                           unsigned char *slot) {
+    const int tid = threadIdx.x;
+    const int n = a.n;
+    {
+        const int r = tid & 127, h = tid >> 7;
+        const int gr = ti * kB + r;
+        if (gr < n) {
+            for (int c = 64 * h; c < 64 * h + 64; ++c) {
+                const int gc = tj * kB + c;
+                if (gc < n) a.LU[(size_t)gr + (size_t)gc * n] = Sp[r * kSp + c];
+            }
+        }
+    }
+#pragma unroll 4
+    for (int u = 0; u < 16; ++u) {
+        const int p = tid + kThreads * u;
+        const int chunk = p >> 10, kg = (p >> 7) & 7, R = ((p >> 3) & 15) * 8 + (p & 7);
+        const int K0 = chunk * 32 + kg * 4;
+        float v[4], hi[4], lo[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            v[q] = bfmt ? Sp[(K0 + q) * kSp + R] : Sp[R * kSp + K0 + q];
+            hi[q] = coop::tc::to_tf32(v[q]);
+            lo[q] = coop::tc::to_tf32(v[q] - hi[q]);
+        }
+        *reinterpret_cast<float4 *>(slot + 16 * (size_t)p) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<float4 *>(slot + kPartBytes + 16 * (size_t)p) =
+            make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
+// In-place Gauss-Jordan inverse of the 128 x 128 tile in Sp (no pivoting):
+// thread (tr, tc) of a 16 x 16 grid keeps rows 8tr.. and columns 8tc.. in
+// registers; per pivot k the owners of column k and row k publish them to
+// shared memory (double-buffered), one barrier, then every thread applies
+//     a_rc <- [c != k] a_rc - L_r U_c  (+1 at r = c = k)
+// with L_r = a_rk (a_kk - 1 at r = k) and U_c = a_kc / a_kk (1 / a_kk at c = k),
+// which is the in-place Gauss-Jordan step.  Returns false (on thread 0) when a
+// pivot is zero or not finite.
+__device__ bool gauss_jordan(float *Sp, float *cbuf, float *rbuf) {
+    const int tid = threadIdx.x;
+    const int tr = tid >> 4, tc = tid & 15;
+    float a[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[i][j] = Sp[(8 * tr + i) * kSp + 8 * tc + j];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const int kb = k >> 3, kl = k & 7;
+        float *cb = cbuf + (k & 1) * kB;
+        float *rb = rbuf + (k & 1) * kB;
+        if (tc == kb) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) cb[8 * tr + i] = a[i][kl];
+        }
+        if (tr == kb) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) rb[8 * tc + j] = a[kl][j];
+        }
+        __syncthreads();
+        const float akk = rb[k];
+        const float p = 1.0f / akk;
+        if (tid == 0 && !(isfinite(p) && akk != 0.f)) ok = false;
+        float L[8], U[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) L[i] = cb[8 * tr + i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) U[j] = rb[8 * tc + j] * p;
+        if (tc == kb) U[kl] = p;
+        if (tr == kb) L[kl] = akk - 1.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (j == kl)
+                    a[i][j] = (tc == kb) ? -L[i] * U[j] : fmaf(-L[i], U[j], a[i][j]);
+                else
+                    a[i][j] = fmaf(-L[i], U[j], a[i][j]);
+            }
+        }
+        if (tr == kb && tc == kb) a[kl][kl] += 1.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) Sp[(8 * tr + i) * kSp + 8 * tc + j] = a[i][j];
+    return ok;
+}
+
+// The A part of the L-tile epilogue's chunk E (S's columns 32E..32E+31, held
+// by the threads of half E / 2) as TF32 hi and lo parts into the chunk's stage.
+template <int E>
+__device__ __forceinline__ void write_a(unsigned char *sm, int g, int row, int half,
+                                        const float (&v)[64]) {
+    if (half != (E >> 1)) return;
+    unsigned char *dst = sm + (size_t)((g + E) % kStages) * kStageBytes;
+    constexpr int c0 = 32 * (E & 1);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        float hi[4], lo[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const float x = v[c0 + 4 * q + w];
+            hi[w] = coop::tc::to_tf32(x);
+            lo[w] = coop::tc::to_tf32(x - hi[w]);
+        }
+        const uint32_t o = poff(row, 4 * q);
+        *reinterpret_cast<float4 *>(dst + o) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<float4 *>(dst + 16384 + o) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + kBarOff);
+    uint64_t *empty = full + kStages;
+    uint64_t *accb = empty + kStages;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kBarOff + 128);
+    int *task_s = reinterpret_cast<int *>(sm + kBarOff + 192);
+    float *Sp = reinterpret_cast<float *>(sm);
+    float *cbuf = Sp + kB * kSp;
+    float *rbuf = cbuf + 2 * kB;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n = a.n, T = a.T;
+    const uint32_t ring = bulk::smem_u32(sm);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
+                         bulk::smem_u32(tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            bulk::init(&full[s], 1);
+            bulk::init(&empty[s], 1);
+        }
+        bulk::init(accb, 1);
+        bulk::fence_init();
+    }
+    coop::tc::fence_before();
+    __syncthreads();
+    coop::tc::fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+    const int row = 32 * (warp & 3) + lane, half = warp >> 2;
+
+    int g = 0;       // chunks filled so far (ring position), same in every thread
+    int naccb = 0;   // completions of accb so far
+    for (;;) {
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+            const int t = atomicAdd(a.ticket, 1);
+            *task_s = (t < T * T && !ld_acq(&a.flags[kFlagBarrierTimeout])) ? a.tasks[t] : -1;
+        }
+        __syncthreads();
+        const int task = *task_s;
+        if (task < 0) break;
+        const int i = task >> 16, j = task & 0xffff, m = min(i, j);
+        // ------------------------------------------------ accumulation over k < m
+        if (m > 0) {
+            if (warp == 0) {
+                if (lane == 0) {
+                    const int total = 4 * m;
+                    auto fill = [&](int c) {
+                        const int gc = g + c, s = gc % kStages;
+                        if (gc >= kStages && !bulk::wait(&empty[s], ((gc - kStages) / kStages) & 1))
+                            gave_up(a.flags);
+                        const int k = c >> 2, q = c & 3;
+                        if (q == 0) {
+                            if (!wait_flag(&a.ready[i * T + k], a.epoch, a.flags)) gave_up(a.flags);
+                            if (!wait_flag(&a.ready[k * T + j], a.epoch, a.flags)) gave_up(a.flags);
+                            fence_async_global();
+                        }
+                        const unsigned char *L = a.op + (size_t)(i * T + k) * kSlotBytes + q * kChunkBytes;
+                        const unsigned char *U = a.op + (size_t)(k * T + j) * kSlotBytes + q * kChunkBytes;
+                        unsigned char *dst = sm + (size_t)s * kStageBytes;
+                        bulk::arrive_expect_tx(&full[s], kStageBytes);
+                        bulk::g2s(dst, L, kChunkBytes, &full[s]);
+                        bulk::g2s(dst + 16384, L + kPartBytes, kChunkBytes, &full[s]);
+                        bulk::g2s(dst + 32768, U, kChunkBytes, &full[s]);
+                        bulk::g2s(dst + 49152, U + kPartBytes, kChunkBytes, &full[s]);
+                    };
+                    fill(0);
+                    if (total > 1) fill(1);
+                    for (int c = 0; c < total; ++c) {
+                        const int gc = g + c, s = gc % kStages;
+                        if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+                        coop::tc::fence_after();
+                        mma_chunk(tmem, ring + s * kStageBytes, c == 0);
+                        coop::tc::commit(bulk::smem_u32(&empty[s]));
+                        if (c + 2 < total) fill(c + 2);
+                    }
+                    coop::tc::commit(bulk::smem_u32(accb));
+                }
+                __syncwarp();
+            }
+            g += 4 * m;
+            if (!bulk::wait(accb, naccb & 1)) gave_up(a.flags);
+            ++naccb;
+            coop::tc::fence_after();
+        }
+        // ------------------------------------------------ S = A_ij - acc (rows `row`, half `half`)
+        float v[64];
+        if (m > 0) {
+            ld64(tmem + lane_base + 64 * half, v);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 64; ++t) v[t] = 0.f;
+        }
+        {
+            const int gr = i * kB + row;
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+                const int gc = j * kB + 64 * half + t;
+                const float av = (gr < n && gc < n) ? a.A[(size_t)gr + (size_t)gc * n]
+                                                    : (gr == gc ? 1.f : 0.f);
+                v[t] = av - v[t];
+            }
+        }
+        unsigned char *slot = a.op + (size_t)(i * T + j) * kSlotBytes;
+        if (i < j) {
+            // U_ij = S
+#pragma unroll
+            for (int t = 0; t < 64; ++t) Sp[row * kSp + 64 * half + t] = v[t];
+            __syncthreads();
+            store_tile(a, Sp, i, j, true, slot);
+        } else if (i == j) {
+#pragma unroll
+            for (int t = 0; t < 64; ++t) Sp[row * kSp + 64 * half + t] = v[t];
+            __syncthreads();
+            const bool ok = gauss_jordan(Sp, cbuf, rbuf);
+            if (tid == 0 && !ok) atomicOr(&a.flags[kFlagSingular], 1);
+            __syncthreads();
+            store_tile(a, Sp, i, j, true, slot);
+        } else {
+            // L_ij = S D_j: four K chunks, A part (S as hi/lo) written by the
+            // threads holding those columns, B part (D_j) copied from its slot
+            const unsigned char *D = a.op + (size_t)(j * T + j) * kSlotBytes;
+            for (int e = 0; e < kStages; ++e) {
+                const int gc = g + e;
+                if (gc >= kStages && !bulk::wait(&empty[gc % kStages], ((gc - kStages) / kStages) & 1))
+                    gave_up(a.flags);
+            }
+            if (tid == 0) {
+                if (!wait_flag(&a.ready[j * T + j], a.epoch, a.flags)) gave_up(a.flags);
+                fence_async_global();
+                for (int e = 0; e < kStages; ++e) {
+                    const int s = (g + e) % kStages;
+                    unsigned char *dst = sm + (size_t)s * kStageBytes;
+                    bulk::arrive_expect_tx(&full[s], 32768);
+                    bulk::g2s(dst + 32768, D + e * kChunkBytes, kChunkBytes, &full[s]);
+                    bulk::g2s(dst + 49152, D + kPartBytes + e * kChunkBytes, kChunkBytes, &full[s]);
+                }
+            }
+            write_a<0>(sm, g, row, half, v);
+            write_a<1>(sm, g, row, half, v);
+            write_a<2>(sm, g, row, half, v);
+            fence_async_shared();
+            __syncthreads();
+            if (tid == 0) {
+                for (int e = 0; e < kStages; ++e) {
+                    const int gc = g + e, s = gc % kStages;
+                    if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+                    coop::tc::fence_after();
+                    mma_chunk(tmem + 128, ring + s * kStageBytes, e == 0);
+                    coop::tc::commit(bulk::smem_u32(&empty[s]));
+                }
+            }
+            // chunk 3 reuses chunk 0's stage once its MMAs are done
+            {
+                const int gc = g + 3, s = gc % kStages;
+                if (!bulk::wait(&empty[s], ((gc - kStages) / kStages) & 1)) gave_up(a.flags);
+                if (tid == 0) {
+                    unsigned char *dst = sm + (size_t)s * kStageBytes;
+                    bulk::arrive_expect_tx(&full[s], 32768);
+                    bulk::g2s(dst + 32768, D + 3 * kChunkBytes, kChunkBytes, &full[s]);
+                    bulk::g2s(dst + 49152, D + kPartBytes + 3 * kChunkBytes, kChunkBytes, &full[s]);
+                }
+                write_a<3>(sm, g, row, half, v);
+                fence_async_shared();
+                __syncthreads();
+                if (tid == 0) {
+                    if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+                    coop::tc::fence_after();
+                    mma_chunk(tmem + 128, ring + s * kStageBytes, false);
+                    coop::tc::commit(bulk::smem_u32(&empty[s]));
+                    coop::tc::commit(bulk::smem_u32(accb));
+                }
+            }
+            g += 4;
+            if (!bulk::wait(accb, naccb & 1)) gave_up(a.flags);
+            ++naccb;
+            coop::tc::fence_after();
+            ld64(tmem + lane_base + 128 + 64 * half, v);
+            // the ring's stages 0-2 may be read by no MMA now: every MMA of this
+            // tile is complete (accb), so the plain tile may overwrite them
+#pragma unroll
+            for (int t = 0; t < 64; ++t) Sp[row * kSp + 64 * half + t] = v[t];
+            __syncthreads();
+            store_tile(a, Sp, i, j, false, slot);
+        }
+        // publish the tile
+        fence_async_global();
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_rel(&a.ready[i * T + j], a.epoch);
+    }
+    coop::tc::fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem)
+                     : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Block triangular solves with the factors in LU (FP32): forward
+// y_i = b_i - sum_{k<i} L_ik y_k, then backward x_i = D_i (y_i - sum_{j>i} U_ij x_j),
+// one CTA per 128-row block, blocks taken from a ticket counter in the order
+// of the dependency chain (forward: i = 0, 1, ...; backward: i = T-1, ...), so
+// no CTA waits for one that has not started.  Thread t keeps rows 2(t%64),
+// 2(t%64)+1 and columns 32(t/64).. of each tile; the next tile's slice is
+// loaded before the wait for the values it multiplies.
+struct SolveArgs {
+    int n, T;
+    const float *LU;
+    const double *b;   // right-hand side (n)
+    float *y, *x;      // T*128 each; x is the solution
+    int *fy, *fx;      // T flags each (== epoch: block done)
+    int *ticket;       // [0] forward, [1] backward tickets (zeroed before the launches)
+    int epoch;
+    int *flags;        // kFlagBarrierTimeout
+};
+
+__device__ __forceinline__ void load_slice(const SolveArgs &s, int ti, int tj, int r2, int cg,
+                                           float2 (&w)[32]) {
+    const int n = s.n;
+    const int gr = ti * kB + 2 * r2;
+#pragma unroll
+    for (int cc = 0; cc < 32; ++cc) {
+        const int gc = tj * kB + 32 * cg + cc;
+        float2 t = make_float2(0.f, 0.f);
+        if (gc < n && gr < n) t = *reinterpret_cast<const float2 *>(s.LU + (size_t)gr + (size_t)gc * n);
+        w[cc] = t;
+    }
+}
+
+template <bool kFwd>
+__global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
+    __shared__ int blk_s;
+    __shared__ float red[4][kB];
+    __shared__ float zs[kB];
+    const int tid = threadIdx.x, r2 = tid & 63, cg = tid >> 6;
+    const int T = s.T;
+    if (tid == 0) {
+        const int t = atomicAdd(&s.ticket[kFwd ? 0 : 1], 1);
+        blk_s = kFwd ? t : T - 1 - t;
+    }
+    __syncthreads();
+    const int i = blk_s;
+    if (i < 0 || i >= T) return;
+    const float *src = kFwd ? s.y : s.x;  // values of the other blocks
+    int *fl = kFwd ? s.fy : s.fx;
+    float acc0 = 0.f, acc1 = 0.f;
+    float2 w[32];
+    const int k_first = kFwd ? 0 : T - 1, k_step = kFwd ? 1 : -1;
+    const int count = kFwd ? i : T - 1 - i;
+    for (int q = 0; q < count; ++q) {
+        const int k = k_first + q * k_step;
+        load_slice(s, i, k, r2, cg, w);
+        if (tid == 0 && !wait_flag(&fl[k], s.epoch, s.flags)) gave_up(s.flags);
+        __syncthreads();
+        const float4 *yv = reinterpret_cast<const float4 *>(src + k * kB + 32 * cg);
+#pragma unroll
+        for (int c4 = 0; c4 < 8; ++c4) {
+            const float4 yy = __ldcg(yv + c4);
+            const float ys[4] = {yy.x, yy.y, yy.z, yy.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                acc0 = fmaf(w[4 * c4 + u].x, ys[u], acc0);
+                acc1 = fmaf(w[4 * c4 + u].y, ys[u], acc1);
+            }
+        }
+    }
+    if (!kFwd) load_slice(s, i, i, r2, cg, w);  // D_i, before the reduction
+    red[cg][2 * r2] = acc0;
+    red[cg][2 * r2 + 1] = acc1;
+    __syncthreads();
+    if (tid < kB) {
+        const int gr = i * kB + tid;
+        float base;
+        if (kFwd)
+            base = gr < s.n ? (float)s.b[gr] : 0.f;
+        else
+            base = s.y[gr];
+        const float z = base - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+        if (kFwd)
+            s.y[gr] = z;
+        else
+            zs[tid] = z;
+    }
+    if (!kFwd) {
+        __syncthreads();
+        acc0 = acc1 = 0.f;
+#pragma unroll
+        for (int cc = 0; cc < 32; ++cc) {
+            const float zz = zs[32 * cg + cc];
+            acc0 = fmaf(w[cc].x, zz, acc0);
+            acc1 = fmaf(w[cc].y, zz, acc1);
+        }
+        __syncthreads();
+        red[cg][2 * r2] = acc0;
+        red[cg][2 * r2 + 1] = acc1;
+        __syncthreads();
+        if (tid < kB)
+            s.x[i * kB + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_rel(&fl[i], s.epoch);
+}
+
+// Self-test of the bounded waits: the cooperative LU's grid barrier with a CTA
+// that never arrives (which = 0), and the block LU's tile-flag wait on a flag
+// that nothing sets (which = 1).  Both give up after their normal poll limits
+// and record kFlagBarrierTimeout.
+__global__ void k_wait_selftest(int which, unsigned *bar, int *flags, int *flag) {
+    __shared__ int dead_s;
+    if (threadIdx.x == 0) dead_s = 0;
+    __syncthreads();
+    if (which == 0) {
+        if (blockIdx.x != 0) return;  // the CTA that never arrives
+        unsigned gen = 0;
+        coop::grid_barrier(bar, flags, gen, &dead_s);
+    } else if (threadIdx.x == 0) {
+        wait_flag(flag, 1, flags);
+    }
+}
+
+}  // namespace blu
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+int blu_tiles(int n) { return (n + blu::kB - 1) / blu::kB; }
+
+size_t blu_op_bytes(int n) {
+    const size_t T = (size_t)blu_tiles(n);
+    return T * T * blu::kSlotBytes;
+}
+
+// The schedule: ring m = min(i, j) ascending; in a ring the diagonal tile, then
+// (m+d, m) and (m, m+d) for d = 1, 2, ...
+std::vector<int> blu_schedule(int n) {
+    const int T = blu_tiles(n);
+    std::vector<int> t;
+    t.reserve((size_t)T * T);
+    for (int m = 0; m < T; ++m) {
+        t.push_back((m << 16) | m);
+        for (int d = 1; m + d < T; ++d) {
+            t.push_back(((m + d) << 16) | m);
+            t.push_back((m << 16) | (m + d));
+        }
+    }
+    return t;
+}
+
+void blu_alloc(BluBufs &B, int n, const int *tasks, BluState *state) {
+    const int T = blu_tiles(n);
+    D4_CUDA_OK(d4::dmalloc((void **)&B.op, blu_op_bytes(n)));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.ticket, sizeof(int) * 4));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.ready, sizeof(int) * (size_t)T * T));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.fy, sizeof(int) * (size_t)T));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.fx, sizeof(int) * (size_t)T));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.y, sizeof(float) * (size_t)T * blu::kB));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.xs, sizeof(float) * (size_t)T * blu::kB));
+    D4_CUDA_OK(cudaMemset(B.ready, 0, sizeof(int) * (size_t)T * T));
+    D4_CUDA_OK(cudaMemset(B.fy, 0, sizeof(int) * (size_t)T));
+    D4_CUDA_OK(cudaMemset(B.fx, 0, sizeof(int) * (size_t)T));
+    D4_CUDA_OK(cudaMemset(B.xs, 0, sizeof(float) * (size_t)T * blu::kB));
+    B.tasks = tasks;
+    B.state = state;
+}
+
+void blu_free(BluBufs &B) {
+    void *p[] = {B.op, B.ticket, B.ready, B.fy, B.fx, B.y, B.xs};
+    for (void *q : p)
+        if (q) cudaFree(q);
+    B = BluBufs();
+}
+
+static bool g_blu_attr = false;
+
+void blu_factor_async(const BluBufs &B, int n, const float *A, float *LU, int *flags, int grid,
+                      cudaStream_t st) {
+    if (!g_blu_attr) {
+        D4_CUDA_OK(cudaFuncSetAttribute(blu::k_blu32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)blu::kSmemBytes));
+        g_blu_attr = true;
+    }
+    const int T = blu_tiles(n);
+    blu::Args a;
+    a.n = n;
+    a.T = T;
+    a.A = A;
+    a.LU = LU;
+    a.op = B.op;
+    a.tasks = B.tasks;
+    a.ticket = B.ticket;
+    a.ready = B.ready;
+    a.epoch = ++B.state->lu_epoch;
+    a.flags = flags;
+    D4_CUDA_OK(cudaMemsetAsync(B.ticket, 0, sizeof(int), st));
+    const int g = std::max(1, std::min(grid, T * T));
+    blu::k_blu32<<<g, blu::kThreads, blu::kSmemBytes, st>>>(a);
+    check_launch("k_blu32");
+}
+
+void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, int *flags,
+                     cudaStream_t st) {
+    const int T = blu_tiles(n);
+    blu::SolveArgs s;
+    s.n = n;
+    s.T = T;
+    s.LU = LU;
+    s.b = b;
+    s.y = B.y;
+    s.x = B.xs;
+    s.fy = B.fy;
+    s.fx = B.fx;
+    s.ticket = B.ticket + 1;
+    s.epoch = ++B.state->solve_epoch;
+    s.flags = flags;
+    D4_CUDA_OK(cudaMemsetAsync(B.ticket + 1, 0, 2 * sizeof(int), st));
+    blu::k_bsolve32<true><<<T, blu::kThreads, 0, st>>>(s);
+    check_launch("k_bsolve32<fwd>");
+    blu::k_bsolve32<false><<<T, blu::kThreads, 0, st>>>(s);
+    check_launch("k_bsolve32<bwd>");
+}
+
+int wait_selftest(int which) {
+    unsigned *bar = nullptr;
+    int *flags = nullptr;
+    D4_CUDA_OK(dmalloc(&bar, sizeof(unsigned) * 64));
+    D4_CUDA_OK(dmalloc(&flags, sizeof(int) * (kFlagCount + 1)));
+    D4_CUDA_OK(cudaMemset(bar, 0, sizeof(unsigned) * 64));
+    D4_CUDA_OK(cudaMemset(flags, 0, sizeof(int) * (kFlagCount + 1)));
+    blu::k_wait_selftest<<<which == 0 ? 2 : 1, 32>>>(which, bar, flags, flags + kFlagCount);
+    check_launch("k_wait_selftest");
+    int h[kFlagCount];
+    const cudaError_t e = cudaMemcpy(h, flags, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(bar);
+    cudaFree(flags);
+    D4_CUDA_OK(e);
+    return h[kFlagBarrierTimeout] ? D4_ERR_STATE : D4_OK;
+}
+
+}  // namespace d4

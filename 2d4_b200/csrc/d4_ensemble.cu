@@ -521,6 +521,8 @@ struct Ensemble {
     int solve_smem = 0;
     long long launches = 0;
     long long vtot = 0;  // entries of each per-dislocation vector pool
+    int pair_ty = 8;     // threads per pair tile along j (autotuned, first run)
+    bool tuned = false;
 };
 
 void check(const char *name) {
@@ -560,7 +562,7 @@ void set_active(Ensemble &E, const std::vector<int> &active) {
 template <bool kJac>
 void sweep(Ensemble &E, int xsel, double hmul, int ea, int eb, int va, int vb) {
     const int na = (int)E.act.size();
-    k_ens_pairs<kJac><<<E.pre_pair[na], dim3(kTile, 8), 0, E.stream>>>(
+    k_ens_pairs<kJac><<<E.pre_pair[na], dim3(kTile, E.pair_ty), 0, E.stream>>>(
         E.P, E.d_ins, E.d_sc, E.d_act, E.d_pre_pair, na, E.cm, xsel, hmul);
     check("k_ens_pairs");
     constexpr int bytes = row_smem_bytes<kJac>();
@@ -572,6 +574,47 @@ void sweep(Ensemble &E, int xsel, double hmul, int ea, int eb, int va, int vb) {
                                                                  E.d_pre_mat, na);
         check("k_ens_matrix<scale>");
     }
+}
+
+// Pair-tile autotuner of the ensemble: threads per tile from the candidates,
+// by timing the stress and fused pair kernels of every active instance
+// (tolerances off; F and A are scratch that every attempt rewrites), one
+// untimed and three timed runs each; the fastest total wins.  Each pair is
+// evaluated by one thread whatever the choice, so results do not depend on it.
+void autotune(Ensemble &E) {
+    if (E.tuned || E.act.empty()) return;
+    Common cm = E.cm;
+    cm.use_dipole = 0;
+    const int na = (int)E.act.size();
+    float best = 1e30f;
+    int best_ty = 8;
+    cudaEvent_t e0, e1;  // own events: E.ev0 times the whole d4_ensemble_run call
+    D4_CUDA_OK(cudaEventCreate(&e0));
+    D4_CUDA_OK(cudaEventCreate(&e1));
+    for (int ty : kPairTyCandidates) {
+        float total = 0;
+        for (int rep = 0; rep < 4; ++rep) {
+            D4_CUDA_OK(cudaEventRecord(e0, E.stream));
+            k_ens_pairs<false><<<E.pre_pair[na], dim3(kTile, ty), 0, E.stream>>>(
+                E.P, E.d_ins, E.d_sc, E.d_act, E.d_pre_pair, na, cm, kX0, 1.0);
+            k_ens_pairs<true><<<E.pre_pair[na], dim3(kTile, ty), 0, E.stream>>>(
+                E.P, E.d_ins, E.d_sc, E.d_act, E.d_pre_pair, na, cm, kX0, 1.0);
+            check("k_ens_pairs<tune>");
+            D4_CUDA_OK(cudaEventRecord(e1, E.stream));
+            D4_CUDA_OK(cudaEventSynchronize(e1));
+            float ms = 0;
+            D4_CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) total += ms;
+        }
+        if (total < best) {
+            best = total;
+            best_ty = ty;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    E.pair_ty = best_ty;
+    E.tuned = true;
 }
 
 void lu(Ensemble &E) {
@@ -691,30 +734,30 @@ int d4_ensemble_create(void **out, int count, const int *n, const d4_params *p) 
         }
         E->vtot = voff;
         for (int v = 0; v < kNumVec; ++v) {
-            D4_CUDA_OK(cudaMalloc((void **)&E->P.v[v], sizeof(double) * voff));
+            D4_CUDA_OK(d4::dmalloc((void **)&E->P.v[v], sizeof(double) * voff));
             D4_CUDA_OK(cudaMemsetAsync(E->P.v[v], 0, sizeof(double) * voff, E->stream));
         }
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.F, sizeof(double) * moff));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.A, sizeof(double) * moff));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.LU, sizeof(double) * moff));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.F, sizeof(double) * moff));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.A, sizeof(double) * moff));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.LU, sizeof(double) * moff));
         D4_CUDA_OK(cudaMemsetAsync(E->P.A, 0, sizeof(double) * moff, E->stream));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.piv, sizeof(int) * voff));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.sing, sizeof(int) * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.sing_any, sizeof(int) * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.ratio, sizeof(double) * 2 * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.strain, sizeof(double) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.piv, sizeof(int) * voff));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.sing, sizeof(int) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.sing_any, sizeof(int) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.ratio, sizeof(double) * 2 * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.strain, sizeof(double) * count));
         D4_CUDA_OK(cudaMemsetAsync(E->P.strain, 0, sizeof(double) * count, E->stream));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.acc, sizeof(int) * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->P.err, sizeof(int) * 4));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.acc, sizeof(int) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->P.err, sizeof(int) * 4));
         D4_CUDA_OK(cudaMemsetAsync(E->P.err, 0, sizeof(int) * 4, E->stream));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_ins, sizeof(Inst) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_ins, sizeof(Inst) * count));
         D4_CUDA_OK(cudaMemcpyAsync(E->d_ins, E->hins.data(), sizeof(Inst) * count,
                                    cudaMemcpyHostToDevice, E->stream));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_sc, sizeof(Sc) * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_act, sizeof(int) * count));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_pre_pair, sizeof(int) * (count + 1)));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_pre_row, sizeof(int) * (count + 1)));
-        D4_CUDA_OK(cudaMalloc((void **)&E->d_pre_mat, sizeof(int) * (count + 1)));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_sc, sizeof(Sc) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_act, sizeof(int) * count));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_pre_pair, sizeof(int) * (count + 1)));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_pre_row, sizeof(int) * (count + 1)));
+        D4_CUDA_OK(d4::dmalloc((void **)&E->d_pre_mat, sizeof(int) * (count + 1)));
         E->hsc.resize(count);
         E->solve_smem = (int)(sizeof(double) * smax);
         D4_CUDA_OK(cudaFuncSetAttribute(k_ens_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -758,10 +801,23 @@ const char *d4_ensemble_last_error(void *ens) {
     return E ? E->err.c_str() : "null ensemble";
 }
 
+int d4_ensemble_pair_tile_threads(void *ens, int *threads_y) {
+    Ensemble *E = (Ensemble *)ens;
+    if (!E || !threads_y) return D4_ERR_ARG;
+    *threads_y = E->tuned ? E->pair_ty : 0;
+    return D4_OK;
+}
+
 int d4_ensemble_set_positions(void *ens, int k, const double *x, const double *y) {
     Ensemble *E = (Ensemble *)ens;
     if (!E || k < 0 || k >= E->count || !x || !y) return D4_ERR_ARG;
     const d4::ens::Inst &in = E->hins[k];
+    const int bad = d4_check_positions(in.n, x, y);
+    if (bad >= 0) {
+        E->err = "d4_ensemble_set_positions: instance " + std::to_string(k) + ", dislocation " +
+                 std::to_string(bad) + " is not finite or outside the cell [-0.5, 0.5)^2";
+        return D4_ERR_ARG;
+    }
     const size_t b = sizeof(double) * in.n;
     if (cudaMemcpy(E->P.v[d4::ens::kX0] + in.voff, x, b, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(E->P.v[d4::ens::kY] + in.voff, y, b, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -811,6 +867,10 @@ int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res) {
                 sweep<false>(*E, kX0, 0, 0, 0, kVI, 0);
             }
         }
+        if (!E->tuned) {
+            if (E->act.empty()) set_active(*E, active);
+            autotune(*E);
+        }
         std::vector<double> ratio(2 * E->count);
         std::vector<int> acc(E->count);
         long long rounds = 0;
@@ -854,6 +914,9 @@ int d4_ensemble_run(void *ens, long long max_rounds, d4_run_result *res) {
                 const int idx = (int)ratio[2 * k + 1];
                 if (idx >= 0) h.selected_id = idx;
                 const double r = ratio[2 * k] / E->dipole_prec_sq;
+                if (!std::isfinite(r))  // as d4_run: stop instead of doubling h forever
+                    throw d4::StateError("non-finite error ratio: an instance's positions or "
+                                         "speeds are not finite");
                 ++h.attempts;
                 h.singular += sing[k] != 0;
                 acc[k] = r < 1;

@@ -158,8 +158,13 @@ __device__ __forceinline__ double xy_diff_x(double dx, double dy, const Hyp &h, 
            f_dx_l(dx - 4, c, h.chm4, h.chm4) + g3;
 }
 
-// normalize, src/sim_utils.cpp:6-13 (while-loop wrap into [-0.5, 0.5)).
+// normalize, src/sim_utils.cpp:6-13 (while-loop wrap into [-0.5, 0.5)).  The
+// loops take at most a few turns for the differences of positions in the cell;
+// a value that is not finite, or so large that n -+ 1 == n, would keep them
+// turning forever (the reference's loops too), so such values skip the loops:
+// infinities and NaN give NaN, the large finite values wrap by rounding.
 __device__ __forceinline__ double normalize(double n) {
+    if (!(fabs(n) < 1048576.0)) return n - rint(n);  // inf - inf and NaN give NaN
     while (n < -0.5) n += 1;
     while (n >= 0.5) n -= 1;
     return n;

@@ -2,7 +2,9 @@
 // with --fmad=false).  The pair tiles and the ordered row sums live in
 // d4_sweep64.cuh.
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "d4_sweep64.cuh"
 
@@ -151,9 +153,9 @@ void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const do
     PairArgs a = pair_args(c, x, y);
     a.F = F;
     if (c.tab)
-        k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, st>>>(a);
+        k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
     else
-        k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, 8), 0, st>>>(a);
+        k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
     check_launch("k_pairs64<speeds>");
     RowArgs r{};
     r.n = c.n;
@@ -173,9 +175,9 @@ void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a
     PairArgs a = pair_args(c, x, y);
     a.h = h;
     if (c.tab)
-        k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+        k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);
     else
-        k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, 8), 0, c.stream>>>(a);
+        k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);
     check_launch("k_pairs64<jacobian>");
     RowArgs r{};
     r.n = c.n;
@@ -194,6 +196,64 @@ void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a
     k_scale_rows64<<<blocks((long long)c.n * c.n, 256), 256, 0, c.stream>>>(c.n, c.A, c.rowsub,
                                                                            c.rowsc);
     check_launch("k_scale_rows64");
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tune_cache;  // (device, n, table) -> threads y
+}  // namespace
+
+// Each candidate runs the stress and the fused pair kernels (tolerances off,
+// writing only the context's scratch F and A) once untimed and three times
+// timed with CUDA events on the context's stream; the fastest total wins.
+void autotune_pairs(Ctx &c) {
+    if (c.pair_tuned) return;
+    int dev = 0;
+    D4_CUDA_OK(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, c.n, c.tab ? c.tab_T : 0);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            c.pair_ty = it->second;
+            c.pair_tuned = true;
+            return;
+        }
+    }
+    PairArgs a = pair_args(c, c.x0, c.y);
+    a.tol = nullptr;
+    a.F = c.F;
+    a.A = c.A;
+    a.h = c.step_size;
+    float best = 1e30f;
+    int best_ty = 8;
+    for (int ty : kPairTyCandidates) {
+        float total = 0;
+        for (int rep = 0; rep < 4; ++rep) {
+            D4_CUDA_OK(cudaEventRecord(c.ev0, c.stream));
+            if (c.tab) {
+                k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, ty), 0, c.stream>>>(a);
+                k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, ty), 0, c.stream>>>(a);
+            } else {
+                k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, ty), 0, c.stream>>>(a);
+                k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, ty), 0, c.stream>>>(a);
+            }
+            check_launch("k_pairs64<tune>");
+            D4_CUDA_OK(cudaEventRecord(c.ev1, c.stream));
+            D4_CUDA_OK(cudaEventSynchronize(c.ev1));
+            float ms = 0;
+            D4_CUDA_OK(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+            if (rep > 0) total += ms;
+        }
+        if (total < best) {
+            best = total;
+            best_ty = ty;
+        }
+    }
+    c.pair_ty = best_ty;
+    c.pair_tuned = true;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best_ty;
 }
 
 void jacobian_from_prev64(Ctx &c, double factor) {
@@ -274,13 +334,36 @@ void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double 
 // overlap on the GPU (different streams, or different host threads) race on
 // it and must be serialised by the caller.  The first call on a device looks
 // up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture begins.
+// current; make that first call before any stream capture begins.  The
+// address is cached per device together with the device's current CUDA
+// context: after a device reset (a new primary context, in which the module
+// is loaded again and the array may move) the next call looks it up again,
+// so that call, too, must come before any capture.
 static __device__ __align__(256) double g_noalloc_pair_force[D4_NOALLOC_MAX_N * D4_NOALLOC_MAX_N];
 
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double *g_noalloc_addr[kMaxDevices] = {};
+void *g_noalloc_ctx[kMaxDevices] = {};
+
+// The calling thread's current CUDA context (the driver's cuCtxGetCurrent,
+// reached through the runtime's entry-point query, so the library needs no
+// link against the driver library); null when it cannot be queried.
+void *current_context() {
+    using Fn = int (*)(void **);
+    static Fn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return reinterpret_cast<Fn>(p);
+    }();
+    void *ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 }  // namespace
 
 extern "C" int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress,
@@ -292,11 +375,13 @@ extern "C" int d4_speeds_noalloc(int n, const double *x, const double *y, double
     double *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        void *ctx = current_context();
+        if (!g_noalloc_addr[dev] || ctx != g_noalloc_ctx[dev]) {
             void *p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_pair_force) != cudaSuccess || !p)
                 return D4_ERR_CUDA;
             g_noalloc_addr[dev] = static_cast<double *>(p);
+            g_noalloc_ctx[dev] = ctx;
         }
         scratch = g_noalloc_addr[dev];
     }

@@ -38,6 +38,26 @@ struct LuBufs {
     int *flags = nullptr, *perm = nullptr, *piv = nullptr;
 };
 
+// Launch counters of one block-LU buffer set (host side): epochs of its tile
+// and solve flags.
+struct BluState {
+    int lu_epoch = 0, solve_epoch = 0;
+};
+
+// Buffers of the mixed form's block LU and block solves (d4_blu32.cu): the
+// packed tensor-core operands of every tile (TF32 hi and lo parts), the
+// schedule, ticket counters ([0] factorisation, [1] forward, [2] backward
+// solve), the tile flags, the solves' block flags and padded vectors.
+struct BluBufs {
+    unsigned char *op = nullptr;
+    const int *tasks = nullptr;
+    int *ticket = nullptr;
+    int *ready = nullptr;
+    int *fy = nullptr, *fx = nullptr;
+    float *y = nullptr, *xs = nullptr;
+    BluState *state = nullptr;
+};
+
 // Buffers of one FP32 factorisation and its refined solves (mixed form): the
 // matrix the refinement's residual multiplies, the factors and the pivot
 // bookkeeping, the refinement vectors and the ring of residual maxima.
@@ -50,6 +70,8 @@ struct Mix32Bufs {
     float *c32 = nullptr, *w1 = nullptr;
     unsigned long long *resid = nullptr;  // 8 pairs (max |r|, max |g|)
     int *resid_count = nullptr;           // host: next slot of resid
+    BluBufs blu;                          // block LU path (Ctx::m_fast)
+    int *blk = nullptr;                   // host: LU32 holds block-LU factors (else pivoted)
 };
 
 // Buffers of the solves of one stage chain: the weights read by the
@@ -67,6 +89,7 @@ struct RunState {
     long long aval_count = 0;
     bool in_aval = false;
     unsigned sub_counter = 0;
+    double wall_start = 0, wall_last = 0;  // log columns 14 and 10 (seconds)
 };
 
 struct Prof {
@@ -135,6 +158,16 @@ struct Ctx {
     unsigned long long *m_resid = nullptr;  // 8 pairs (max |r|, max |g|) of recent solves
     int m_resid_count = 0;
     int ir_iters = 2;
+    // block LU path of the mixed form (d4_blu32.cu): on by default; an attempt
+    // whose block factorisation met a bad pivot, or whose refined residual
+    // stayed above kRefineLimit, is redone with the pivoted cooperative LU
+    int m_fast = 1;
+    int *blu_tasks = nullptr;
+    BluBufs blu;  // the primary buffer set's block-LU buffers
+    BluState blu_state, blu_state_b;
+    int m_blk = 0, m_blk_b = 0;  // Mix32Bufs::blk of the primary and stage-I buffer sets
+    long long m_blocklu = 0, m_fallbacks = 0;
+    double m_worst_refine = 0;
 
     // cutoff sparse path: CSR of the matrix and the GMRES work space
     int use_gmres = 0;
@@ -172,6 +205,10 @@ struct Ctx {
     double *m_vacc_b = nullptr;
     int m_resid_count_b = 0;
 
+    // pair-tile autotuner (FP64 pair kernels): threads per 32x32 tile along j
+    int pair_ty = 8;
+    bool pair_tuned = false;
+
     RunState rs;
     Prof prof;
 };
@@ -191,6 +228,15 @@ struct ProfScope {
 };
 
 extern std::atomic<long long> g_launches;
+extern std::atomic<long long> g_allocs;
+
+// Every device allocation of the library goes through this wrapper, which
+// counts it (d4_device_allocations).
+template <typename T>
+inline cudaError_t dmalloc(T **p, size_t bytes) {
+    g_allocs.fetch_add(1, std::memory_order_relaxed);
+    return cudaMalloc((void **)p, bytes);
+}
 
 // ---- FP64 pair sweeps (d4_fp64.cu) ----
 // Stress sweep: F (signed pair forces) and tolerance update, then ordered row sums.
@@ -207,6 +253,13 @@ void normalize64(Ctx &c, double *x_dst, const double *x_src);
 void strain_increment64(Ctx &c, const double *x_old, const double *x_new, double *out);
 void field_eval64(Ctx &c, int count, const double *dx, const double *dy, double *xy,
                   double *xyd);
+
+// Pair-tile autotuner (d4_fp64.cu): picks the threads per pair tile of the FP64
+// pair kernels by timing the candidates on the context's positions, once per
+// (device, n, field) in the process; results do not depend on the choice.
+void autotune_pairs(Ctx &c);
+// The candidates and the timing shared with the ensemble's tuner.
+constexpr int kPairTyCandidates[3] = {2, 4, 8};
 
 // ---- FP64 factorisation and solves (d4_lu64.cu) ----
 // Factorises A into LU; returns via flags whether the pivoted path ran and
@@ -235,6 +288,10 @@ void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const do
                    double ext, double *v);
 // Plain solve of A dx = g (g on device, dx written to c.dx).
 void solve_plain64(Ctx &c, const double *g);
+// Mixed form: refined solve of A32 dx = g with the last factorisation (g on
+// device, dx written to c.dx); the block LU's factorisation falls back to the
+// pivoted one by itself when a diagonal tile met a bad pivot (factor32).
+void solve_plain32(Ctx &c, const double *g);
 
 // ---- mixed form (d4_mixed.cu) ----
 void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v);
@@ -258,6 +315,25 @@ void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const do
                    const double *y, double ext, double *v);
 int factor32(Ctx &c);
 int coop_grid_size32(int n);
+
+// ---- mixed form's block LU (d4_blu32.cu) ----
+constexpr double kRefineLimit = 1e-9;  // refined max|r| / max|g| above this: exact path
+int blu_tiles(int n);
+size_t blu_op_bytes(int n);
+std::vector<int> blu_schedule(int n);
+void blu_alloc(BluBufs &B, int n, const int *tasks, BluState *state);
+void blu_free(BluBufs &B);
+// Factorises A (FP32, column-major n x n) into LU (block factors, plain) and the
+// packed operands of B, on `st` with up to `grid` CTAs; flags receives
+// kFlagSingular (a diagonal tile's Gauss-Jordan met a bad pivot) and
+// kFlagBarrierTimeout (a bounded wait gave up).
+void blu_factor_async(const BluBufs &B, int n, const float *A, float *LU, int *flags, int grid,
+                      cudaStream_t st);
+// Runs a bounded wait on a barrier or flag that nothing completes (d4_wait_selftest).
+int wait_selftest(int which);
+// x = (block LU)^-1 b in FP32 (b FP64); the result is B.xs (padded to 128-row blocks).
+void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, int *flags,
+                     cudaStream_t st);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
 

@@ -1,8 +1,12 @@
 // d4_mixed.cu: the mixed-precision form of the implicit step.
 //
-// Pair stress and gradient in FP32 (d4_field32.cuh: compensated image sums,
+// Pair stress gradient in FP32 (d4_field32.cuh: compensated image sums,
 // cancellation-free central image), each unique pair once per sweep, summed
-// into FP64 accumulators.  The dense Jacobian A = I + D J is kept in FP32 and
+// into FP64 accumulators.  The pair stress itself, whose sums are the speeds
+// that enter the Newton residual g, is the FP64 field: speeds from the FP32
+// field (about 1e-6 relative) moved positions by 1.9e-8 from the FP64 form
+// within 8 steps at N=4096, while the gradient only shapes the matrix, whose
+// error the refined solves remove.  The dense Jacobian A = I + D J is kept in FP32 and
 // factorised in FP32 (the cooperative LU of d4_lu_coop.cuh).  FP64 is kept for
 // positions, speeds, residuals g, d_i, the position updates and the error ratio;
 // each solve is refined in FP64 against the stored FP32 matrix:
@@ -87,11 +91,14 @@ __global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
                 row_min = fmin(row_min, dist_sq);
                 tol_min(a.tol, j, dist_sq);
             }
-            float s, sd;
-            f32::field<kJac>((float)dx, (float)dy, s, sd);
+            // the force enters the Newton residual: FP64 field (an FP32 force,
+            // ~1e-6 relative, moved positions by ~1e-8 within a few steps)
             const double bj = bsign(j, a.n);
-            f = (double)s * bi * bj;
+            f = f64::xy(dx, dy, f64::Hyp(f64::exp2pix(dx)), f64::cos2piy(dy)) * bi * bj;
             if (kJac && dist_sq < a.range_sq * a.cut_sq) {
+                // the gradient only builds the matrix: FP32, compensated
+                float s, sd;
+                f32::field<true>((float)dx, (float)dy, s, sd);
                 double vv = a.h * bj * bi * (double)sd;
                 if (!a.heaviside && dist_sq > a.cut_sq) {
                     const double t = sqrt(dist_sq) - a.cutoff;
@@ -354,6 +361,8 @@ Mix32Bufs primary_mix32(Ctx &c) {
     B.w1 = c.m_w1;
     B.resid = c.m_resid;
     B.resid_count = &c.m_resid_count;
+    B.blu = c.blu;
+    B.blk = &c.m_blk;
     return B;
 }
 
@@ -361,6 +370,16 @@ void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix
                     cudaStream_t st, cudaEvent_t after_copy) {
     const int n = c.n;
     const size_t bytes = sizeof(float) * (size_t)n * n;
+    *B.blk = c.m_fast;
+    if (c.m_fast) {
+        // block LU (d4_blu32.cu): reads the matrix, writes the factors and operands
+        D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
+        if (copy_matrix) D4_CUDA_OK(cudaMemcpyAsync(B.A32, A, bytes, cudaMemcpyDeviceToDevice, st));
+        if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
+        blu_factor_async(B.blu, n, copy_matrix ? B.A32 : A, B.LU32, B.flags, grid, st);
+        ++c.m_blocklu;
+        return;
+    }
     D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
     D4_CUDA_OK(cudaMemsetAsync(B.bar, 0, sizeof(unsigned) * 64, st));
     D4_CUDA_OK(cudaMemsetAsync(B.mask, 0, sizeof(unsigned) * c.lu_mask_words, st));
@@ -390,6 +409,22 @@ int factor32(Ctx &c) {
                                cudaMemcpyDeviceToHost, c.stream));
     D4_CUDA_OK(cudaStreamSynchronize(c.stream));
     if (c.h_flags[kFlagBarrierTimeout]) throw StateError("LU grid barrier timed out");
+    if (c.m_blk && c.h_flags[kFlagSingular]) {
+        // a diagonal tile met a zero or non-finite pivot: the pivoted LU instead
+        ++c.m_fallbacks;
+        c.m_fast = 0;
+        try {
+            factor32_async(c, primary_mix32(c), c.A32, false, c.lu32_grid, c.stream, nullptr);
+        } catch (...) {
+            c.m_fast = 1;
+            throw;
+        }
+        c.m_fast = 1;
+        D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
+                                   cudaMemcpyDeviceToHost, c.stream));
+        D4_CUDA_OK(cudaStreamSynchronize(c.stream));
+        if (c.h_flags[kFlagBarrierTimeout]) throw StateError("LU grid barrier timed out");
+    }
     count_lu(c, c.h_flags);
     c.factor_singular = c.h_flags[kFlagSingular] != 0;
     c.factor_pivoted = 0;
@@ -409,13 +444,20 @@ int coop_grid_size32(int n) {
     return g < (n + coop::kThreads - 1) / coop::kThreads ? -1 : g;
 }
 
-// FP32 cluster solve with B's factors: out = LU32^-1 r (r FP64 in, out FP32).
-static void solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const double *r,
-                         float *out) {
+// FP32 solve with B's factors: LU32^-1 r (r FP64 in, result FP32), by the
+// block solves of the block LU, or by the cluster solve of the pivoted LU.
+// Returns the result's buffer.
+static const float *solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const double *r) {
+    if (*B.blk) {
+        blu_solve_async(B.blu, c.n, B.LU32, r, B.flags, st);
+        return B.blu.xs;
+    }
     trsv::GArgs g{};
     g.gmode = -1;
     g.g_in = r;
-    trsv::launch_cluster_solve<float>(c.n, B.LU32, B.perm, B.flags, g, B.w1, out, c.wave_err, st);
+    trsv::launch_cluster_solve<float>(c.n, B.LU32, B.perm, B.flags, g, B.w1, B.c32, c.wave_err,
+                                      st);
+    return B.c32;
 }
 
 void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
@@ -435,8 +477,8 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
     check_launch("k_ir_init");
     const int chunk = 256;
     for (int it = 0; it < c.ir_iters; ++it) {
-        solve32_once(c, B, st, B.r, B.c32);
-        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, B.c32, B.dx);
+        const float *corr = solve32_once(c, B, st, B.r);
+        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, corr, B.dx);
         check_launch("k_ir_accum");
         k_gemv_part32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(n, B.A32, B.dx, B.part,
                                                                       chunk);
@@ -449,6 +491,32 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
     *B.resid_count = (*B.resid_count + 1) % 8;
     k_ir_apply<<<nb(n, 256), 256, 0, st>>>(n, B.dx, B.flags, base, out, dx_out);
     check_launch("k_ir_apply");
+}
+
+void solve_plain32(Ctx &c, const double *g) {
+    const int n = c.n;
+    Mix32Bufs B = primary_mix32(c);
+    trsv::GArgs ga{};
+    ga.gmode = -1;
+    ga.g_in = g;
+    k_ir_init<<<nb(n, 256), 256, 0, c.stream>>>(n, ga, B.g, B.r, B.dx);
+    check_launch("k_ir_init");
+    const int chunk = 256;
+    for (int it = 0; it < c.ir_iters; ++it) {
+        const float *corr = solve32_once(c, B, c.stream, B.r);
+        k_ir_accum<<<nb(n, 256), 256, 0, c.stream>>>(n, corr, B.dx);
+        check_launch("k_ir_accum");
+        k_gemv_part32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, c.stream>>>(n, B.A32, B.dx,
+                                                                             B.part, chunk);
+        check_launch("k_gemv_part32");
+        k_resid32<<<nb(n, 256), 256, 0, c.stream>>>(n, B.g, B.part, nb(n, chunk), B.r);
+        check_launch("k_resid32");
+    }
+    k_absmax2<<<64, 256, 0, c.stream>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
+    check_launch("k_absmax2");
+    *B.resid_count = (*B.resid_count + 1) % 8;
+    D4_CUDA_OK(cudaMemcpyAsync(c.dx, B.dx, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                               c.stream));
 }
 
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,

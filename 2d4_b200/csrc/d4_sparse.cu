@@ -343,15 +343,15 @@ void sparse_alloc(Ctx &c) {
     c.sp_grid = std::max(1, std::min(sms, sp::nb(n, 128)));
     if (sp::nb(n, c.sp_grid) > sp::kThreads) throw StateError("n too large for the GMRES grid");
     c.sp_nch = sp::nb(n, sp::kChunk);
-    auto ialloc = [](int **p, size_t k) { D4_CUDA_OK(cudaMalloc((void **)p, sizeof(int) * k)); };
+    auto ialloc = [](int **p, size_t k) { D4_CUDA_OK(d4::dmalloc((void **)p, sizeof(int) * k)); };
     auto dalloc = [](double **p, size_t k) {
-        D4_CUDA_OK(cudaMalloc((void **)p, sizeof(double) * k));
+        D4_CUDA_OK(d4::dmalloc((void **)p, sizeof(double) * k));
     };
     ialloc(&c.sp_cnt, (size_t)c.sp_nch * n);
     ialloc(&c.sp_off, (size_t)c.sp_nch * n);
     ialloc(&c.sp_rp, (size_t)n + 1);
     ialloc(&c.sp_flags, 4);
-    D4_CUDA_OK(cudaMalloc((void **)&c.sp_bar, sizeof(unsigned) * 64));
+    D4_CUDA_OK(d4::dmalloc((void **)&c.sp_bar, sizeof(unsigned) * 64));
     dalloc(&c.sp_dinv, n);
     dalloc(&c.sp_V, (size_t)(sp::kM + 1) * n);
     dalloc(&c.sp_z, n);
@@ -395,8 +395,8 @@ void sparse_prepare(Ctx &c) {
         c.sp_ci = nullptr;
         c.sp_val = nullptr;
         c.sp_cap = nnz + nnz / 4 + 1024;
-        D4_CUDA_OK(cudaMalloc((void **)&c.sp_ci, sizeof(int) * (size_t)c.sp_cap));
-        D4_CUDA_OK(cudaMalloc((void **)&c.sp_val, sizeof(double) * (size_t)c.sp_cap));
+        D4_CUDA_OK(d4::dmalloc((void **)&c.sp_ci, sizeof(int) * (size_t)c.sp_cap));
+        D4_CUDA_OK(d4::dmalloc((void **)&c.sp_val, sizeof(double) * (size_t)c.sp_cap));
     }
     c.sp_nnz = nnz;
     if (mixed)

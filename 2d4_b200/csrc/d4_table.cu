@@ -70,7 +70,7 @@ __global__ void k_table_build(int T, int W, double2 *t) {
 
 void table_build(Ctx &c) {
     const int T = c.tab_T, W = T + 1 + 2 * tab::kGuard;
-    D4_CUDA_OK(cudaMalloc((void **)&c.tab, sizeof(double2) * (size_t)W * W));
+    D4_CUDA_OK(d4::dmalloc((void **)&c.tab, sizeof(double2) * (size_t)W * W));
     k_table_build<<<dim3((W + 127) / 128, W), 128, 0, c.stream>>>(T, W, c.tab);
     check_launch("k_table_build");
 }

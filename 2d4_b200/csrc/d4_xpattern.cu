@@ -141,10 +141,10 @@ extern "C" int d4_xpattern_df(int n, const double *x, const double *y, const int
         return e == cudaSuccess;
     };
     const size_t tab = (size_t)std::max(n, 1) * K;
-    if (ok(cudaMalloc(&dv, sizeof(double) * 2 * std::max(n, 1))) &&
-        ok(cudaMalloc(&ex, sizeof(double2) * tab)) && ok(cudaMalloc(&ey, sizeof(double2) * tab)) &&
-        ok(cudaMalloc(&dnrm, sizeof(double) * 4 * (size_t)K * K)) &&
-        ok(cudaMalloc(&dacc, sizeof(double) * 4 * K))) {
+    if (ok(d4::dmalloc(&dv, sizeof(double) * 2 * std::max(n, 1))) &&
+        ok(d4::dmalloc(&ex, sizeof(double2) * tab)) && ok(d4::dmalloc(&ey, sizeof(double2) * tab)) &&
+        ok(d4::dmalloc(&dnrm, sizeof(double) * 4 * (size_t)K * K)) &&
+        ok(d4::dmalloc(&dacc, sizeof(double) * 4 * K))) {
         if (n > 0) {
             ok(cudaMemcpy(dv, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
             ok(cudaMemcpy(dv + n, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice));

@@ -106,3 +106,33 @@ def gather_results(local_idx, local_rows, count, group=None):
             local_rows, dtype=torch.float64, device=dev)
     dist.all_reduce(full, group=group)
     return full.cpu().numpy()
+
+
+def run_sharded(sd, configs, max_rounds=0, group=None, device=None, ensemble_cls=None):
+    """The ensemble sharded over the ranks of a torch.distributed process group
+    (one process per GPU): rank r runs the instances ``partition(ns, world)[r]``
+    as one ``Ensemble`` on its own device, with no data-path exchange; at the
+    end one all_reduce (``gather_results``) gives every rank every instance's
+    results.  Returns (results rows in instance order, {instance: (x, y)} for
+    this rank's instances).  Every rank makes the same collective call, also a
+    rank that owns no instance.  ``ensemble_cls`` stands in for ``Ensemble``
+    (same constructor, run, positions and close)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    ns = [len(x) for x, _ in configs]
+    mine = partition(ns, world)[rank]
+    if device is None:
+        device = torch.cuda.current_device() if torch.cuda.is_available() else 0
+    cls = ensemble_cls or Ensemble
+    rows = np.zeros((0, len(RESULT_FIELDS)))
+    positions = {}
+    if mine:
+        ens = cls(sd, [configs[k] for k in mine], device=device)
+        try:
+            rows = results_array(ens.run(max_rounds))
+            positions = {k: ens.positions(j) for j, k in enumerate(mine)}
+        finally:
+            ens.close()
+    return gather_results(mine, rows, len(ns), group), positions

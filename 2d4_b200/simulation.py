@@ -349,6 +349,20 @@ class Engine:
         self._call("d4_lu_stats", *[C.byref(t) for t in v])
         return dict(zip(("factorizations", "passes", "swaps"), [t.value for t in v]))
 
+    def mixed_stats(self):
+        """Mixed form's factorisations (d4_mixed_stats): block LUs run, attempts
+        redone with the pivoted LU, worst refined residual of the block-LU
+        attempts."""
+        b, f, w = C.c_longlong(), C.c_longlong(), C.c_double()
+        self._call("d4_mixed_stats", C.byref(b), C.byref(f), C.byref(w))
+        return {"block_factorizations": b.value, "fallbacks": f.value,
+                "worst_refined_residual": w.value}
+
+    def set_block_lu(self, enable=True):
+        """Mixed form: block LU with per-attempt fallback (default), or always
+        the pivoted cooperative LU (d4_set_block_lu)."""
+        self._call("d4_set_block_lu", int(bool(enable)))
+
     def positions(self):
         x = np.empty(self.n)
         y = np.empty(self.n)

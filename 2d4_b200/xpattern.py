@@ -47,11 +47,14 @@ def direct_fourier(x, y, b, res=1024, acc=None):
 
 
 class ToolExit(Exception):
-    """A stop of the command line: message and exit status."""
+    """A stop of the command line: message and exit status.  The reference
+    tool writes every one of these messages to std::cerr, the unreadable .ini
+    file's too although it then returns 0 (xpattern/xpattern.cpp:76-120), so
+    to_stderr defaults to True."""
 
-    def __init__(self, message, status):
+    def __init__(self, message, status, to_stderr=True):
         super().__init__(message)
-        self.message, self.status = message, status
+        self.message, self.status, self.to_stderr = message, status, to_stderr
 
 
 def input_files(path, out=None):
@@ -128,7 +131,7 @@ def main(argv=None, out=None, err=None):
             raise ToolExit("--create-maps is not built here (only the k spectra of df). "
                            "Program terminates.", 255)
     except ToolExit as e:
-        print(e.message, file=err if e.status else out)
+        print(e.message, file=err if e.to_stderr else out)
         return e.status
     acc = None
     for f in files:

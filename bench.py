@@ -16,10 +16,14 @@ reference itself (tests/golden/c2_relaxed_1024.npz), then constant external
 stress tau = 0.05 (FixedRateProtocol(0.05, 0)) with time and step size reset,
 default precision (-P 1e-5 -p 0.05).  Synthetic seeded data; no dataset.
 
-Timing: W warm-up steps, then K steps, each timed on the device with CUDA
-events around one d4_advance(1) call on the library's stream, with a 512 MiB
-buffer written between steps to flush L2 (the step's working set, ~24 MB, is
-below L2).  Multi-GPU (--gpus N under torchrun): the single system does not
+Timing: W warm-up steps on their own engine; then K accepted steps from the
+workload's start (the same steps the reference arm times), each timed on the
+device with CUDA events around one d4_advance(1) call on the library's stream,
+with a 512 MiB buffer written between steps to flush L2 (the step's working
+set, ~24 MB, is below L2), profiling off.  e2e repeats the same K steps on a
+fresh engine through the public API with host buffers (positions uploaded
+from pinned memory before and read back after each step, wall clock); a third
+pass with per-category CUDA events gives kernel_ms and the roofline.  Multi-GPU (--gpus N under torchrun): the single system does not
 shard (one GPU per system), so each rank runs an independent replica (weak
 scaling); the time is the max over ranks and value = total steps of all ranks x
 N / that time.
@@ -29,7 +33,9 @@ flags (oracle/_ref/libd4ref_fast.so, UMFPACK replaced by OpenBLAS dgetrf/dgetrs 
 all host cores) on the same workload, through Simulation::run, rank 0 only.
 
 At N=1 the line also carries bounded legs for the other configurations:
-mixed_vs_fp64 (N=4096 dense), cutoff (N=4096, Heaviside c = 0.1: FP64 dense,
+mixed_vs_fp64 (N=4096 dense, tau = 0.1, and N=1024 from the relaxed start:
+the two forms in lockstep for --mixed-steps accepted steps, default 1000, with
+the position difference after every step), cutoff (N=4096, Heaviside c = 0.1: FP64 dense,
 FP64 GMRES, mixed GMRES), tabulated (the N=1024 workload with the tabulated
 field), ensemble (512 instances of uneven N), adjoint (N=2048, 200 steps) and
 xpattern (direct-Fourier pattern analysis, N=4096 at resolution 1024).
@@ -50,9 +56,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic work per unit (frozen; counted from the kernel sources, see
-# DESIGN.md): FLOP per unique pair of a stress sweep and of a fused
-# stress + gradient sweep, and the LU/solve counts of a dense N x N system.
+# Algorithmic work per unit (frozen; counted once from the field's expressions,
+# src/Fields/Field.cpp:191-330, each division, exp2 and cos counted as one
+# operation): FLOP per unique pair of a stress sweep and of a fused
+# stress + gradient sweep; the LU and solve counts of a dense N x N system are
+# 2N^3/3 and 2N^2.
 W_STRESS_PAIR = 136
 W_FUSED_PAIR = 386
 
@@ -63,7 +71,91 @@ WORKLOADS = {
                desc="N=64 plain FP64, tau_ext=0, P=1e-8"),
     "c3-fp64": dict(n=4096, tau=0.1, precision=1e-5, source=("seed", 1002),
                     desc="N=4096 plain FP64, dense Jacobian, tau_ext=0.1"),
+    "c4": dict(n=None, tau=0.0, precision=1e-5, source="ensemble",
+               desc="512-instance ensemble, N_k uniform over even values in [64, 2048], "
+                    "tau_ext = 1e-3 t, sharded over the ranks (one ensemble per GPU)"),
 }
+
+
+def ensemble_configs(pkg, count=512, seed=2000):
+    """The ensemble workload's instances: N_k uniform over even values in
+    [64, 2048] (seed 2000), positions seeds 3000 + k, internal order."""
+    rng = np.random.default_rng(seed)
+    ns = (rng.integers(32, 1025, size=count) * 2).tolist()
+    return ns, [pkg.dconf.generate_internal(n, 3000 + k)[:2] for k, n in enumerate(ns)]
+
+
+def run_ensemble_workload(args, wl):
+    """--workload c4: the ensemble sharded over the torchrun ranks (partition
+    by n^3, one Ensemble per GPU, no data-path collective; weak in the
+    instance count per rank only through the partition).  A step is one
+    attempt round; W warm-up rounds (with the initial sweeps), then K rounds
+    timed on the device by the library's CUDA events (d4_ensemble_run's
+    device_seconds), max over ranks; value = accepted dislocation-steps of all
+    ranks / that time.  e2e: the whole sharded run through the public API
+    (ensemble.run_sharded's parts: positions uploaded from host arrays, rounds,
+    per-instance results gathered to every rank), wall clock."""
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module("2d4_b200")
+    ens_mod = importlib.import_module("2d4_b200.ensemble")
+    lib = pkg._lib.load()
+    ns, cfg = ensemble_configs(pkg)
+    mine = ens_mod.partition(ns, ws)[rank]
+    sd = pkg.SimulationData()
+    sd.external_stress = pkg.FixedRateProtocol(0.0, 1e-3)
+    sd.time_limited, sd.time_limit = True, 200.0
+    t0 = time.perf_counter()
+    ens = ens_mod.Ensemble(sd, [cfg[k] for k in mine], device=local)
+    r0 = ens.run(args.warmup)
+    launches0 = lib.d4_kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if ws > 1:
+        dist.barrier()
+    r1 = ens.run(args.steps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = lib.d4_kernel_launches() - launches0
+    dev = r1[0].device_seconds
+    acc = sum(ns[k] * (b.successful_steps - a.successful_steps)
+              for k, a, b in zip(mine, r0, r1))
+    att = sum(ns[k] * (b.attempts - a.attempts) for k, a, b in zip(mine, r0, r1))
+    rows = ens_mod.results_array(r1)
+    ens.close()
+    full = ens_mod.gather_results(mine, rows, len(ns)) if ws > 1 else rows
+    wall = time.perf_counter() - t0
+    t = torch.tensor([dev, wall, acc, att], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        dev, wall, acc, att = float(mx[0]), float(mx[1]), float(sm[2]), float(sm[3])
+    if rank == 0:
+        line = {"metric": "dislocation-steps/s", "value": acc / dev, "unit": "dislocation-steps/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * dev / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": wl["desc"], "instances": len(ns), "sum_n": int(sum(ns)),
+                           "step": "one attempt round of every active instance",
+                           "parallelism": "instances sharded over %d ranks" % ws,
+                           "attempted_dislocation_steps_per_s": att / dev,
+                           "instances_with_results": int(np.count_nonzero(full[:, 5]))},
+                "e2e": {"value": acc / wall, "unit": "dislocation-steps/s",
+                        "h2d_bytes_per_step": int(16 * sum(ns[k] for k in mine) / args.steps),
+                        "d2h_bytes_per_step": int(8 * len(ns) * len(ens_mod.RESULT_FIELDS)),
+                        "note": "wall clock of the whole sharded run (create, upload, warm-up "
+                                "and timed rounds, gather)"},
+                "gpu_launches": int(launches), "clocks": clk}
+        print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
 
 
 def dist_env():
@@ -230,46 +322,83 @@ def roofline(prof, n, hbm_gbs, fp64_tf):
                 peak_source="cuBLAS DGEMM 4096^3 measured in this run (FP64 peak)")
 
 
-def mixed_vs_fp64(pkg, steps=8, warmup=2, n=4096, seed=1002, tau=0.1):
-    """The metric's comparison: N=4096 (seed 1002, tau_ext = 0.1, default
-    precision), the plain FP64 form and the mixed form from the same start,
-    each timed over `steps` accepted steps (CUDA events, device time), and the
-    max position difference between the two after those steps (meaningful when
-    both took the same step sequence, reported as same_steps)."""
-    x, y, _ = pkg.dconf.generate_internal(n, seed)
-    out = {}
+def attempt_roofline(prof, n, mixed, hbm_gbs, fp64_tf, tf32_tf):
+    """Roofline of the dominant kernel category of a profiled pass (per-category
+    CUDA events around each call): algorithmic work per call / mean call time,
+    against the FP64 DGEMM peak (plain form) or the TF32 tensor peak (the mixed
+    form's factorisation), or HBM for the solves."""
+    r = roofline(prof, n, hbm_gbs, fp64_tf)
+    if mixed and r["kernel"] == "factor":
+        r["peak"] = tf32_tf
+        r["frac"] = r["achieved"] / tf32_tf
+        r["peak_source"] = ("half the measured bf16 dense peak (TF32 runs at half the bf16 "
+                            "rate); the 3xTF32 products issue 3 MMAs per product, counted once")
+    return r
+
+
+def mixed_vs_fp64(pkg, n, seed, tau, steps, start=None, report_every=100):
+    """The metric's comparison at one N: the plain FP64 form and the mixed form
+    from the same start, advanced in lockstep one accepted step at a time
+    (device time of each d4_advance by CUDA events), the max periodic
+    |x_mixed - x_fp64| after every step (the mixed form's error against the
+    FP64 form along the same step sequence: both forms must take the same
+    accepted/failed steps, reported as same_steps), and one profiled pass of
+    each form over the first steps for the per-call kernel times."""
+    if start is not None:
+        x, y = start
+    else:
+        x, y, _ = pkg.dconf.generate_internal(n, seed)
+    engs = []
+    for mode in (pkg._lib.D4_PREC_FP64, pkg._lib.D4_PREC_MIXED):
+        sd = pkg.SimulationData()
+        sd.set_positions(x, y)
+        sd.precision_mode = mode
+        sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
+        engs.append(pkg.Engine(sd))
+    t = [0.0, 0.0]
+    att = [0, 0]
+    fail = [0, 0]
+    worst, errs = 0.0, []
+    same = True
+    for s in range(1, steps + 1):
+        for k, e in enumerate(engs):
+            r = e.advance(1)
+            t[k] += r.device_seconds
+            att[k] += int(r.attempts)
+            fail[k] += int(r.failed_steps)
+        same = same and att[0] == att[1]
+        d = pkg.dconf.conf_compare(engs[1].positions()[0], y, engs[0].positions()[0], y)[0]
+        worst = max(worst, d)
+        if s % report_every == 0 or s == steps:
+            errs.append([s, d])
+    ms = engs[1].mixed_stats()
+    for e in engs:
+        e.close()
+    # per-call kernel times: a profiled pass over a few steps from the same start
+    prof = {}
     for name, mode in (("fp64", pkg._lib.D4_PREC_FP64), ("mixed", pkg._lib.D4_PREC_MIXED)):
         sd = pkg.SimulationData()
         sd.set_positions(x, y)
         sd.precision_mode = mode
         sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
-        eng = pkg.Engine(sd)
-        eng.advance(warmup)
-        eng.profile(True)
-        lu0 = eng.lu_stats()
-        r = eng.advance(steps)
-        lu1 = eng.lu_stats()
-        prof = eng.profile_read()
-        nlu = max(lu1["factorizations"] - lu0["factorizations"], 1)
-        out[name] = dict(value=n * steps / r.device_seconds, attempts=int(r.attempts),
-                         failed=int(r.failed_steps), x=eng.positions()[0],
-                         ms_per_call={k: round(v[0] / max(v[1], 1), 3) for k, v in prof.items()},
-                         lu_passes_per_block=(lu1["passes"] - lu0["passes"]) / (nlu * -(-n // 32)),
-                         lu_swaps=(lu1["swaps"] - lu0["swaps"]) / nlu)
-        eng.close()
-    d, _, _, _ = pkg.dconf.conf_compare(out["mixed"]["x"], y, out["fp64"]["x"], y)
-    return {"n": n, "tau_ext": tau, "steps": steps, "warmup": warmup,
-            "fp64_dislocation_steps_per_s": out["fp64"]["value"],
-            "mixed_dislocation_steps_per_s": out["mixed"]["value"],
-            "speedup": out["mixed"]["value"] / out["fp64"]["value"],
-            "same_steps": out["fp64"]["attempts"] == out["mixed"]["attempts"],
-            "attempts": [out["fp64"]["attempts"], out["mixed"]["attempts"]],
-            "max_position_diff_vs_fp64": d,
-            "fp64_ms_per_call": out["fp64"]["ms_per_call"],
-            "mixed_ms_per_call": out["mixed"]["ms_per_call"],
-            "lu_passes_per_block": [out["fp64"]["lu_passes_per_block"],
-                                    out["mixed"]["lu_passes_per_block"]],
-            "lu_swaps_per_factorization": [out["fp64"]["lu_swaps"], out["mixed"]["lu_swaps"]]}
+        e = pkg.Engine(sd)
+        e.advance(1)
+        e.profile(True)
+        e.advance(min(steps, 10))
+        prof[name] = e.profile_read()
+        e.close()
+    return {"n": n, "tau_ext": tau, "steps": steps,
+            "fp64_dislocation_steps_per_s": n * steps / t[0],
+            "mixed_dislocation_steps_per_s": n * steps / t[1],
+            "speedup": t[0] / t[1], "same_steps": same, "attempts": att, "failed": fail,
+            "max_position_diff_vs_fp64": worst, "position_diff_every_%d_steps" % report_every: errs,
+            "mixed_block_factorizations": ms["block_factorizations"],
+            "mixed_fallbacks_to_pivoted_lu": ms["fallbacks"],
+            "mixed_worst_refined_residual": ms["worst_refined_residual"],
+            "fp64_ms_per_call": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof["fp64"].items()},
+            "mixed_ms_per_call": {k: round(v[0] / max(v[1], 1), 4)
+                                  for k, v in prof["mixed"].items()},
+            "_prof": prof}
 
 
 def cutoff_leg(pkg, steps=6, warmup=1, n=4096, seed=1002, tau=0.1, u=6.4):
@@ -366,9 +495,7 @@ def ensemble_leg(pkg, count=512, rounds=3, seed=2000):
     [64, 2048] (seed 2000), positions seeds 3000 + k, tau_ext = 1e-3 t, time
     limit 200; one warm-up round (with the initial sweeps), then `rounds`
     attempt rounds timed on the device."""
-    rng = np.random.default_rng(seed)
-    ns = (rng.integers(32, 1025, size=count) * 2).tolist()
-    cfg = [pkg.dconf.generate_internal(n, 3000 + k)[:2] for k, n in enumerate(ns)]
+    ns, cfg = ensemble_configs(pkg, count, seed)
     sd = pkg.SimulationData()
     sd.external_stress = pkg.FixedRateProtocol(0.0, 1e-3)
     sd.time_limited, sd.time_limit = True, 200.0
@@ -467,7 +594,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the N=4096 mixed vs FP64 leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed vs FP64 legs")
+    ap.add_argument("--mixed-steps", type=int, default=1000,
+                    help="accepted steps of the mixed vs FP64 legs (N=4096 and N=1024)")
     ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint,xpattern",
                     help="extra single-GPU legs (comma list, or 'none')")
     args = ap.parse_args()
@@ -475,6 +604,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference_arm(args, wl)
+    if args.workload == "c4":
+        return run_ensemble_workload(args, wl)
 
     import torch
     ws, rank, local = dist_env()
@@ -489,9 +620,16 @@ def main():
     lib = pkg._lib.load()
     n = wl["n"]
     x, y = start_state(pkg, wl)
-    eng = pkg.Engine(make_sd(pkg, x, y, wl), device=local)
-    for _ in range(args.warmup):
-        eng.advance(1)
+
+    def fresh():
+        return pkg.Engine(make_sd(pkg, x, y, wl), device=local)
+
+    # warm-up on its own engine: every timed pass below starts from the same
+    # state (the workload's start, t = 0, the initial step size), so they time
+    # the same accepted steps as each other and as the reference arm
+    eng = fresh()
+    eng.advance(args.warmup)
+    eng.close()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
     def barrier():
@@ -499,10 +637,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    # (1) value: device time of each d4_advance(1), inputs resident, no profiling
+    eng = fresh()
     clocks = ClockSampler(local)
     launches0 = lib.d4_kernel_launches()
-    lu0 = eng.lu_stats()
-    eng.profile(True)
     clocks.start()
     barrier()
     t_dev, attempts, failed = 0.0, 0, 0
@@ -516,29 +654,44 @@ def main():
     barrier()
     clk = clocks.stop()
     launches = lib.d4_kernel_launches() - launches0
-    lu1 = eng.lu_stats()
-    prof = eng.profile_read()
-    eng.profile(False)
+    x_value = eng.positions()[0]
+    eng.close()
 
-    # end to end through the public API: host positions in, step, host positions out
-    xh = np.empty(n)
-    yh = np.empty(n)
-    eng_x, eng_y = eng.positions()
-    xh[:] = eng_x
-    yh[:] = eng_y
-    pin_x = torch.from_numpy(xh).pin_memory().numpy()
-    pin_y = torch.from_numpy(yh).pin_memory().numpy()
+    # (2) e2e: the same steps through the public API with host buffers: each
+    # step uploads the positions from pinned host memory, steps, and reads
+    # them back (wall clock around the three calls)
+    eng = fresh()
+    pin_x = torch.from_numpy(x.copy()).pin_memory().numpy()
+    pin_y = torch.from_numpy(y.copy()).pin_memory().numpy()
     barrier()
-    t_e2e = 0.0
+    t_e2e, att_e2e, fail_e2e = 0.0, 0, 0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng._call("d4_set_positions", pkg._lib.ptr(pin_x), pkg._lib.ptr(pin_y))
-        eng.advance(1)
+        r = eng.advance(1)
         eng._call("d4_get_positions", pkg._lib.ptr(pin_x), pkg._lib.ptr(pin_y))
         t_e2e += time.perf_counter() - t0
+        att_e2e += r.attempts
+        fail_e2e += r.failed_steps
     barrier()
+    eng.close()
+
+    # (3) a profiled pass over the same steps: per-category CUDA events for
+    # kernel_ms and the roofline (never the timed number)
+    eng = fresh()
+    lu0 = eng.lu_stats()
+    eng.profile(True)
+    att_prof = 0
+    for _ in range(args.steps):
+        att_prof += eng.advance(1).attempts
+    prof = eng.profile_read()
+    eng.profile(False)
+    lu1 = eng.lu_stats()
+    eng.close()
+    same_steps = (att_e2e == attempts and fail_e2e == failed and att_prof == attempts and
+                  bool(np.array_equal(pin_x, x_value)))
 
     t_max, e2e_max = t_dev, t_e2e
     if dist:
@@ -549,7 +702,6 @@ def main():
     value = n * total_steps / t_max
     e2e = n * total_steps / e2e_max
     if rank != 0:
-        eng.close()
         if dist:
             dist.destroy_process_group()
         return
@@ -564,9 +716,12 @@ def main():
             "config": {"workload": wl["desc"], "n": n, "form": "plain FP64",
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "flushed between steps (512 MiB write)",
+                       "timed_steps": "accepted steps 1..K from the workload's start (warm-up "
+                                      "on a separate engine), as the reference arm",
                        "attempts": attempts, "failed_steps": failed},
             "e2e": {"value": e2e, "unit": "dislocation-steps/s",
-                    "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n},
+                    "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 16 * n,
+                    "attempts": att_e2e, "same_steps": same_steps},
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "kernel_ms": {k: v[0] for k, v in prof.items()},
             "kernel_calls": {k: v[1] for k, v in prof.items()}}
@@ -576,10 +731,20 @@ def main():
                       "passes_per_block": (lu1["passes"] - lu0["passes"]) / (nlu * -(-n // 32)),
                       "swaps_per_factorization": (lu1["swaps"] - lu0["swaps"]) / nlu}
     if ws == 1 and not args.no_mixed:
-        try:
-            line["mixed_vs_fp64"] = mixed_vs_fp64(pkg)
-        except Exception as e:  # pragma: no cover
-            line["mixed_vs_fp64"] = {"unavailable": str(e)}
+        tf32_tf = bf16 / 2
+        for key, kw in (("mixed_vs_fp64", dict(n=4096, seed=1002, tau=0.1)),
+                        ("mixed_vs_fp64_n1024", dict(n=1024, seed=1001, tau=0.05,
+                                                     start=start_state(pkg, WORKLOADS["c2"])))):
+            try:
+                leg = mixed_vs_fp64(pkg, steps=args.mixed_steps, **kw)
+                pr = leg.pop("_prof")
+                leg["roofline_mixed"] = attempt_roofline(pr["mixed"], kw["n"], True, hbm,
+                                                         fp64_tf, tf32_tf)
+                leg["roofline_fp64"] = attempt_roofline(pr["fp64"], kw["n"], False, hbm,
+                                                        fp64_tf, tf32_tf)
+                line[key] = leg
+            except Exception as e:  # pragma: no cover
+                line[key] = {"unavailable": str(e)}
     legs = [] if args.legs == "none" else args.legs.split(",")
     for name, fn in (("cutoff", lambda: cutoff_leg(pkg)),
                      ("tabulated", lambda: tabulated_leg(pkg, wl)),
@@ -604,7 +769,6 @@ def main():
         except Exception as e:  # pragma: no cover
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     print(json.dumps(line))
-    eng.close()
     if dist:
         dist.destroy_process_group()
 

@@ -158,7 +158,16 @@ int d4_create(void **ctx, int n, const d4_params *p);
 int d4_destroy(void *ctx);
 const char *d4_last_error(void *ctx);
 
+/* Positions must be finite and inside the cell [-0.5, 0.5)^2 (where the
+ * reference's normalize keeps them, src/sim_utils.cpp:6-13); d4_set_positions
+ * and d4_ensemble_set_positions reject others with D4_ERR_ARG.  d4_run,
+ * d4_advance and d4_ensemble_run return D4_ERR_STATE when an attempt's error
+ * ratio is not finite, where the reference (without its DEBUG_VERSION checks,
+ * src/simulation.cpp:754-948) would fail every attempt while doubling h. */
 int d4_set_positions(void *ctx, const double *x, const double *y);
+/* The check itself: the index of the first offending dislocation, -1 when all
+ * n are valid (-2 for bad arguments).  No device work. */
+int d4_check_positions(int n, const double *x, const double *y);
 int d4_get_positions(void *ctx, double *x, double *y);
 int d4_set_time(void *ctx, double sim_time, double step_size);
 
@@ -179,17 +188,20 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
 int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *dvec);
 
 /* Replace the device matrix by a dense column-major n x n matrix (the
- * umfpack_di_numeric input of src/simulation.cpp:638, expanded from CSC). */
+ * umfpack_di_numeric input of src/simulation.cpp:638, expanded from CSC).  The
+ * mixed form stores it rounded to FP32. */
 int d4_set_matrix(void *ctx, const double *a_colmajor);
 
 /* Factorise the device Jacobian.  Returns D4_WARN_SINGULAR on an exact zero
- * pivot, like umfpack_di_numeric. */
+ * pivot, like umfpack_di_numeric.  Mixed form: the block LU, or the pivoted
+ * FP32 LU when a diagonal tile met a zero or non-finite pivot. */
 int d4_factor(void *ctx);
 
 /* Solve A dx = g with the last factorisation (UMFPACK_A).  Returns
  * D4_WARN_SINGULAR like umfpack_di_solve and, like it, leaves the result as
  * computed; d4_attempt/d4_run apply solveEQSys's zeroing of entries outside
- * (-1, 1) (src/simulation.cpp:646-658) themselves. */
+ * (-1, 1) (src/simulation.cpp:646-658) themselves.  Mixed form: the FP32
+ * factors' solve refined in FP64 against the FP32 matrix. */
 int d4_solve(void *ctx, const double *g, double *dx);
 
 /* Reset the per-dislocation tolerances (PrecisionHandler::reset). */
@@ -233,6 +245,29 @@ int d4_solver_stats(void *ctx, long long *solves, long long *iterations, long lo
  * (pivots off the diagonal).  No counterpart in the reference. */
 int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long long *swaps);
 
+/* Mixed form's factorisations (no counterpart in the reference): block LU
+ * factorisations run (128 x 128 tiles on the tensor cores, no row interchanges
+ * between tiles), attempts redone with the pivoted cooperative LU because a
+ * diagonal tile met a zero or non-finite pivot or a refined residual stayed
+ * above 1e-9 (max|g - A dx| / max|g|), and the worst refined residual of the
+ * block-LU attempts. */
+int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
+                   double *worst_refined);
+
+/* Pair-tile autotuner (no counterpart in the reference): the FP64 form's pair
+ * kernels evaluate each 32 x 32 tile of pairs with 32 x threads_y threads;
+ * the first d4_run or d4_advance on a context picks threads_y from {2, 4, 8}
+ * by timing each on the context's positions (once per device, n and field in
+ * the process; the results do not depend on the choice).  threads_y = 0 until
+ * then. */
+int d4_pair_tile_threads(void *ctx, int *threads_y);
+
+/* Mixed form: enable = 1 (the default) factorises with the block LU and
+ * falls back per attempt as d4_mixed_stats describes; 0 always uses the
+ * pivoted cooperative LU (exact partial pivoting, as the FP64 form).  No
+ * counterpart in the reference. */
+int d4_set_block_lu(void *ctx, int enable);
+
 /* Batched ensemble of independent systems: the many-realisation statistics
  * workload, where the reference runs one system per process
  * (src/simulation.cpp:30-281).  FP64 form, analytic field, dense LU; every
@@ -250,6 +285,9 @@ int d4_ensemble_create(void **ens, int count, const int *n, const d4_params *p);
 int d4_ensemble_destroy(void *ens);
 const char *d4_ensemble_last_error(void *ens);
 int d4_ensemble_set_positions(void *ens, int k, const double *x, const double *y);
+/* The ensemble's pair-tile autotuner (as d4_pair_tile_threads, over all the
+ * active instances at the first d4_ensemble_run; 0 until then). */
+int d4_ensemble_pair_tile_threads(void *ens, int *threads_y);
 int d4_ensemble_get_positions(void *ens, int k, double *x, double *y);
 /* Runs attempt rounds until no instance is active or max_rounds rounds
  * (<= 0: no cap) have run in this call; may be called again to continue.
@@ -315,12 +353,25 @@ int d4_adjoint(void *ctx, long long steps, const double *t0s, const double *hs,
 /* Number of kernels this library has launched in the process so far. */
 long long d4_kernel_launches(void);
 
+/* Self-test of the kernels' bounded waits (no counterpart in the reference):
+ * which = 0 runs the cooperative LU's grid barrier with one CTA that never
+ * arrives, which = 1 the block LU's tile-flag wait on a flag that nothing
+ * sets.  The wait gives up after its normal limit (about a second), the
+ * kernel records the timeout and returns, and the call returns D4_ERR_STATE
+ * (D4_OK would mean the wait did not give up); the context stays usable. */
+int d4_wait_selftest(void *ctx, int which);
+
+/* Number of device allocations (cudaMalloc) this library has made in the
+ * process so far.  No counterpart in the reference. */
+long long d4_device_allocations(void);
+
 /* Allocation-free FP64 stress sweep (no counterpart in the reference: an
  * addition of this library).  For callers that cannot allocate device memory,
  * such as code running under CUDA-graph stream capture, real-time loops that
  * must not wait on an allocator, or hosts whose device memory belongs to
- * another framework's allocator.  Same result as d4_speeds: speeds v[n] and the
- * tolerance update of tol[n] (may be null; starts from the caller's values,
+ * another framework's allocator.  Same result as d4_speeds of an FP64 context
+ * with the analytic field (no table; the mixed form sums its pairs in another
+ * order): speeds v[n] and the tolerance update of tol[n] (may be null; starts from the caller's values,
  * clamped below min_prec_sq as PrecisionHandler::updateTolerance does) for
  * positions x[n], y[n] in internal order at external stress ext_stress.  All
  * pointers are DEVICE pointers owned by the caller; the work is queued on
@@ -329,8 +380,10 @@ long long d4_kernel_launches(void);
  * D4_NOALLOC_MAX_N^2 doubles (8 MiB) that every GPU loading the library holds
  * until exit: n > D4_NOALLOC_MAX_N is rejected with D4_ERR_ARG, as are odd n.
  * The first call on a device looks the array up (cudaGetSymbolAddress) and
- * must come before any stream capture; calls share the array, so calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * must come before any stream capture; so must the first call after a device
+ * reset, which looks it up again (the address is cached per device and CUDA
+ * context).  Calls share the array, so calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 #define D4_NOALLOC_MAX_N 1024
 int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress, double *v,
                       double *tol, double min_prec_sq, void *stream);

@@ -63,7 +63,11 @@ class RParams(C.Structure):
         ("calculate_strain", C.c_int), ("calculate_order_parameter", C.c_int),
         ("const_external_stress", C.c_double), ("has_rate", C.c_int), ("rate", C.c_double),
         ("has_cyclic", C.c_int), ("cyclic_period", C.c_double),
-        ("has_amplitude_rate", C.c_int), ("amplitude_rate", C.c_double)]
+        ("has_amplitude_rate", C.c_int), ("amplitude_rate", C.c_double),
+        ("sub_config_path", C.c_char_p), ("sub_config_delay", C.c_uint),
+        ("sub_config_delay_during_avalanche", C.c_uint), ("sub_config_times", C.c_double),
+        ("sub_config_times_type", C.c_char), ("avalanche_limit", C.c_longlong),
+        ("avalanche_speed_threshold", C.c_double)]
 
 
 class RResult(C.Structure):
@@ -198,9 +202,10 @@ class Reference:
         p = RParams()
         self.L.d4ref_default_params(C.byref(p))
         for k, v in kw.items():
-            if k == "weight_function":
+            if k in ("weight_function", "sub_config_times_type", "sub_config_path"):
                 v = v.encode()
             setattr(p, k, v)
+        p._keep = [getattr(p, "sub_config_path")]  # the path's bytes live as long as p
         return p
 
     def load(self, path, cap=1 << 20):

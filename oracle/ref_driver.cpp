@@ -50,6 +50,13 @@ extern "C" void d4ref_default_params(d4ref_params *p) {
     p->step_count_limit = -1;
     p->strain_increase_limit = -1;
     p->const_external_stress = 0;
+    p->sub_config_path = nullptr;
+    p->sub_config_delay = 5;
+    p->sub_config_delay_during_avalanche = 1;
+    p->sub_config_times = 0;
+    p->sub_config_times_type = 'a';
+    p->avalanche_limit = -1;
+    p->avalanche_speed_threshold = 1e-3;
 }
 
 namespace {
@@ -85,6 +92,20 @@ std::shared_ptr<SimulationData> make_data(const char *in_path, const d4ref_param
     if (p->step_count_limit >= 0) {
         sD->isStepCountLimit = true;
         sD->stepCountLimit = (unsigned int)p->step_count_limit;
+    }
+    if (p->avalanche_limit >= 0) {  // src/project_parser.cpp:244-249
+        sD->countAvalanches = true;
+        sD->avalancheTriggerLimit = (unsigned int)p->avalanche_limit;
+        sD->avalancheSpeedThreshold = p->avalanche_speed_threshold;
+    }
+    if (p->sub_config_path) {  // src/project_parser.cpp:251-276
+        sD->isSaveSubConfigs = true;
+        sD->subConfigPath = p->sub_config_path;
+        sD->subConfigDelay = p->sub_config_delay;
+        sD->subConfigTimesType = p->sub_config_times_type;
+        sD->subConfigTimes = p->sub_config_times > 0 ? p->sub_config_times : 0;
+        sD->subConfigDelayDuringAvalanche = p->sub_config_delay_during_avalanche;
+        sD->nextWriteOutTime = sD->getNextWriteOutTime();
     }
     const double s = p->const_external_stress;
     if (p->has_amplitude_rate && p->has_cyclic && p->has_rate)

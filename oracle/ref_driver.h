@@ -40,6 +40,13 @@ typedef struct d4ref_params {
     double cyclic_period;       /* -i */
     int has_amplitude_rate;     /* -A given */
     double amplitude_rate;      /* -A */
+    const char *sub_config_path; /* -o (null: not given) */
+    unsigned sub_config_delay;  /* -N, default 5 */
+    unsigned sub_config_delay_during_avalanche; /* -n, default 1 */
+    double sub_config_times;    /* -T, <= 0: not given */
+    char sub_config_times_type; /* -b, default 'a' */
+    long long avalanche_limit;  /* --avalanche-detection-limit, < 0: not given */
+    double avalanche_speed_threshold; /* default 1e-3 */
 } d4ref_params;
 
 typedef struct d4ref_result {

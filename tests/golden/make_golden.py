@@ -27,7 +27,20 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import pyoracle  # noqa: E402
 
 dconf = importlib.import_module("2d4_b200.dconf")
-REF_FIXTURE = "/root/reference/init_config_gen/README_files/1000_64.dconf"
+
+
+def reference_root():
+    """The reference tree: $D4_REFERENCE_ROOT, else the oracle recipe's default."""
+    import subprocess
+    env = os.environ.get("D4_REFERENCE_ROOT")
+    if env:
+        return env
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref-root"],
+                       capture_output=True, text=True, check=True)
+    return r.stdout.strip()
+
+
+REF_FIXTURE = os.path.join(reference_root(), "init_config_gen", "README_files", "1000_64.dconf")
 
 
 def parse_log(path):

@@ -66,3 +66,69 @@ def test_gather_two_gloo_ranks(tmp_path):
     owner = {k: r for r, p in enumerate(e.partition(ns, 2)) for k in p}
     for k in range(len(ns)):
         assert a0[k, 0] == k + 0.5 and a0[k, 3] == k and a0[k, 7] == owner[k]
+
+
+class StubEnsemble:
+    """Stands in for Ensemble on CPU: deterministic per-instance results from
+    the instance's own positions, so the gathered rows show which instances
+    each rank ran."""
+
+    def __init__(self, sd, configs, device=0):
+        self.configs = configs
+
+    def run(self, max_rounds=0):
+        import types
+        out = []
+        for x, y in self.configs:
+            out.append(types.SimpleNamespace(
+                sim_time=float(np.sum(x)), step_size=1e-6, strain=float(np.sum(y)),
+                successful_steps=len(x), failed_steps=max_rounds, attempts=len(x) + max_rounds,
+                singular_factorizations=0, device_seconds=0.25))
+        return out
+
+    def positions(self, j):
+        return self.configs[j]
+
+    def close(self):
+        pass
+
+
+def _sharded_main(rank, world, port, out_dir):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    e = ens_mod()
+    rng = np.random.default_rng(2000)
+    ns = (rng.integers(2, 40, size=11) * 2).tolist()
+    configs = [(np.random.default_rng(3000 + k).uniform(-0.5, 0.5, n),
+                np.random.default_rng(4000 + k).uniform(-0.5, 0.5, n)) for k, n in enumerate(ns)]
+    full, pos = e.run_sharded(None, configs, max_rounds=3, ensemble_cls=StubEnsemble)
+    np.save(os.path.join(out_dir, "full%d.npy" % rank), full)
+    np.save(os.path.join(out_dir, "mine%d.npy" % rank), np.array(sorted(pos)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_run_sharded_two_gloo_ranks(tmp_path):
+    """partition -> one ensemble per rank -> gather_results, composed by
+    run_sharded: every rank ends with every instance's row, each computed by
+    exactly the rank that owns the instance."""
+    import torch.multiprocessing as mp
+    e = ens_mod()
+    port = _free_port()
+    mp.start_processes(_sharded_main, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    f0, f1 = np.load(tmp_path / "full0.npy"), np.load(tmp_path / "full1.npy")
+    assert np.array_equal(f0, f1)
+    rng = np.random.default_rng(2000)
+    ns = (rng.integers(2, 40, size=11) * 2).tolist()
+    parts = e.partition(ns, 2)
+    assert sorted(np.load(tmp_path / "mine0.npy").tolist()) == parts[0]
+    assert sorted(np.load(tmp_path / "mine1.npy").tolist()) == parts[1]
+    for k, n in enumerate(ns):
+        x = np.random.default_rng(3000 + k).uniform(-0.5, 0.5, n)
+        assert f0[k, 0] == np.sum(x) and f0[k, 3] == n and f0[k, 4] == 3

@@ -1,10 +1,13 @@
 """GPU checks of the mixed-precision form against the FP64 oracle (marked gpu).
 
-FP32 pair stress/gradient with compensated image sums, FP32 Jacobian and LU,
-FP64 residuals, refinement, positions and acceptance.  Tolerances: per-pair
-FP32 rounding (~1e-7 relative) for the sweeps and the matrix; the refined solve
-to 1e-10 relative residual; one attempt's positions to 1e-8; a fixed step
-sequence of 200 accepted steps to 1e-7 against the plain FP64 form.
+FP32 pair gradient with compensated image sums and FP32 Jacobian, block LU on
+the tensor cores; FP64 speeds (the residual's pair stress), residuals,
+refinement, positions and acceptance.  Tolerances: the speeds to 1e-12
+relative (FP64 field, pair sums in another order than the reference's); the
+matrix to per-pair FP32 rounding (~1e-7 relative); the refined solve to 1e-10
+relative residual; one attempt's positions to 1e-10; 1000 accepted steps of the
+headline workload to 1e-8 against the plain FP64 form along the same step
+sequence, the bound the mixed form is built to.
 """
 import numpy as np
 import pytest
@@ -30,13 +33,12 @@ def test_mixed_speeds(pkg, restated, n, seed):
     mps, _, _, _ = restated.derived(p, n)
     tol_o = np.full(n, mps)
     vo = restated.speeds(x, y, 0.0, tol_o, mps)
-    assert np.abs(v - vo).max() / np.abs(vo).max() < 1e-6
+    assert np.abs(v - vo).max() / np.abs(vo).max() < 1e-12
     assert np.array_equal(tol, tol_o)  # distances stay FP64
 
 
 def test_mixed_close_pairs(pkg, golden):
-    """Near-field pairs (r^2 <= 1e-6 uses the reference's Taylor branch): the
-    half-angle FP32 form keeps ~1e-6 relative accuracy there."""
+    """Near-field pairs (r^2 <= 1e-6 uses the reference's Taylor branch)."""
     x = np.array([0.1, 0.1 + 3e-4, -0.2, 0.3])
     y = np.array([0.05, 0.05 - 2e-4, 0.2, -0.1])
     import pyoracle
@@ -44,7 +46,7 @@ def test_mixed_close_pairs(pkg, golden):
     vo = ro.speeds(x, y, 0.0)
     e = engine(pkg, x, y)
     v, _ = e.speeds(x, y, 0.0)
-    assert np.abs(v - vo).max() / np.abs(vo).max() < 2e-6
+    assert np.abs(v - vo).max() / np.abs(vo).max() < 1e-12
 
 
 def test_mixed_jacobian(pkg, restated):
@@ -67,8 +69,8 @@ def test_mixed_attempt(pkg, restated, n, h):
     p = restated.params(protocol=dict(kind=1, tau0=0.1, rate=0.0))
     mps, _, _, _ = restated.derived(p, n)
     xbo, xho, x2o, _, ro, io = restated.attempt(x, y, 0.0, h, p, np.full(n, mps))
-    assert np.abs(x2 - x2o).max() < 1e-8
-    assert np.abs(xb - xbo).max() < 1e-8
+    assert np.abs(x2 - x2o).max() < 1e-10
+    assert np.abs(xb - xbo).max() < 1e-10
     assert r.refine_residual < 1e-10
     assert ro < 1  # a step size the error control accepts
     assert abs(r.ratio - ro) <= 1e-3 * ro + 1e-12
@@ -97,3 +99,33 @@ def test_mixed_fixed_steps_vs_fp64(pkg):
     assert out[0][1].failed_steps == out[1][1].failed_steps
     d, _, _, _ = pkg.dconf.conf_compare(out[1][0], y, out[0][0], y)
     assert d < 1e-7
+
+
+def test_mixed_1000_steps_vs_fp64(pkg):
+    """The headline workload (N=1024 relaxed by the reference, constant stress
+    0.05), 1000 accepted steps of both forms in lockstep: the same accepted and
+    failed steps, and the mixed positions within 1e-8 of the FP64 form's after
+    every step."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "c2_relaxed_1024.npz"))
+    x, y = z["x"], z["y"]
+    engs = []
+    for mode in (pkg._lib.D4_PREC_FP64, pkg._lib.D4_PREC_MIXED):
+        sd = pkg.SimulationData()
+        sd.set_positions(x, y)
+        sd.precision_mode = mode
+        sd.external_stress = pkg.FixedRateProtocol(0.05, 0.0)
+        engs.append(pkg.Engine(sd))
+    worst = 0.0
+    for s in range(1000):
+        r64 = engs[0].advance(1)
+        rmx = engs[1].advance(1)
+        assert (r64.attempts, r64.failed_steps) == (rmx.attempts, rmx.failed_steps), s
+        d = pkg.dconf.conf_compare(engs[1].positions()[0], y, engs[0].positions()[0], y)[0]
+        worst = max(worst, d)
+    assert worst <= 1e-8, worst
+    st = engs[1].mixed_stats()
+    assert st["block_factorizations"] > 0 and st["worst_refined_residual"] < 1e-9
+    for e in engs:
+        e.close()

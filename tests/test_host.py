@@ -189,3 +189,19 @@ def test_size_limits_rejected_before_device_work(pkg):
         for k, v in kw.items():
             setattr(p, k, v)
         assert lib.d4_ensemble_create(C.byref(ens), 2, arr, C.byref(p)) == -1, kw
+
+
+def test_position_check(pkg):
+    """d4_check_positions (used by d4_set_positions and
+    d4_ensemble_set_positions): finite values inside [-0.5, 0.5)^2 only."""
+    lib = pkg._lib.load()
+    x = np.linspace(-0.5, 0.49, 8)
+    y = np.zeros(8)
+    assert lib.d4_check_positions(8, pkg._lib.ptr(x), pkg._lib.ptr(y)) == -1
+    for bad in (np.nan, np.inf, -np.inf, 0.5, -0.5000001, 3.0):
+        for arr in ("x", "y"):
+            xx, yy = x.copy(), y.copy()
+            (xx if arr == "x" else yy)[5] = bad
+            assert lib.d4_check_positions(8, pkg._lib.ptr(xx), pkg._lib.ptr(yy)) == 5
+    assert lib.d4_check_positions(0, None, None) == -1
+    assert lib.d4_check_positions(-1, None, None) == -2

@@ -70,6 +70,11 @@ def test_cli_options_and_checks(tmp_path):
     assert st == 1 and "Not enough input files" in msg
     st, msg = run(["-i", str(tmp_path / "none.ini"), "-m", "df"])
     assert st == 0 and "couldn't open" in msg
+    # like every other check's message, the reference writes this one to
+    # std::cerr although it returns 0 (xpattern/xpattern.cpp:88-91)
+    out, err = io.StringIO(), io.StringIO()
+    assert xp.main(["-i", str(tmp_path / "none.ini"), "-m", "df"], out, err) == 0
+    assert "couldn't open" in err.getvalue() and out.getvalue() == ""
 
 
 def test_input_list(tmp_path):

@@ -50,6 +50,7 @@ def test_speeds_noalloc_matches_speeds(pkg):
                      torch.empty(n, dtype=torch.float64, device=dev),
                      torch.full((n,), min_prec_sq, dtype=torch.float64, device=dev)))
     torch.cuda.synchronize()
+    allocs_before = lib.d4_device_allocations()
     free_before = torch.cuda.mem_get_info(dev)[0]
     for (n, _), (xd, yd, vd, td), (v_ref, tol_ref) in zip(cases, bufs, expected):
         st = lib.d4_speeds_noalloc(n, xd.data_ptr(), yd.data_ptr(), C.c_double(0.0),
@@ -59,7 +60,11 @@ def test_speeds_noalloc_matches_speeds(pkg):
         v = vd.cpu().numpy()
         assert rel_err(v, v_ref) < 1e-11
         assert np.array_equal(td.cpu().numpy(), tol_ref)
-    assert torch.cuda.mem_get_info(dev)[0] == free_before  # nothing allocated
+    # nothing allocated: the library's own allocation counter is unchanged;
+    # the device's free memory, which other processes and lazily loaded
+    # modules can also change, is a secondary check within 2 MiB
+    assert lib.d4_device_allocations() == allocs_before
+    assert abs(torch.cuda.mem_get_info(dev)[0] - free_before) <= 2 * 1024 * 1024
 
 
 def test_speeds_noalloc_rejects_sizes(pkg):
