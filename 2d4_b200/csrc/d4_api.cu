@@ -1070,7 +1070,10 @@ int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, doub
     const size_t b = sizeof(double) * (size_t)count;
     cudaMemcpyAsync(d, dx, b, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(d + count, dy, b, cudaMemcpyHostToDevice, c->stream);
-    d4::field_eval64(*c, count, d, d + count, d + 2 * count, d + 3 * count);
+    if (c->p.precision == D4_PREC_MIXED)
+        d4::field_eval_mixed(*c, count, d, d + count, d + 2 * count, d + 3 * count);
+    else
+        d4::field_eval64(*c, count, d, d + count, d + 2 * count, d + 3 * count);
     cudaMemcpyAsync(xy, d + 2 * count, b, cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(xyd, d + 3 * count, b, cudaMemcpyDeviceToHost, c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);

@@ -472,7 +472,7 @@ struct SolveArgs {
     const double *b;   // right-hand side (n)
     float *y, *x;      // T*128 each; x is the solution
     int *fy, *fx;      // T flags each (== epoch: block done)
-    int *ticket;       // [0] forward, [1] backward tickets (zeroed before the launches)
+    int *ticket;       // ticket counter (zeroed before the launch)
     int epoch;
     int *flags;        // kFlagBarrierTimeout
 };
@@ -490,20 +490,12 @@ __device__ __forceinline__ void load_slice(const SolveArgs &s, int ti, int tj, i
     }
 }
 
+// One row block of the forward (kFwd) or backward pass.
 template <bool kFwd>
-__global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
-    __shared__ int blk_s;
-    __shared__ float red[4][kB];
-    __shared__ float zs[kB];
+__device__ __forceinline__ void solve_block(const SolveArgs &s, int i, float (*red)[kB],
+                                            float *zs) {
     const int tid = threadIdx.x, r2 = tid & 63, cg = tid >> 6;
     const int T = s.T;
-    if (tid == 0) {
-        const int t = atomicAdd(&s.ticket[kFwd ? 0 : 1], 1);
-        blk_s = kFwd ? t : T - 1 - t;
-    }
-    __syncthreads();
-    const int i = blk_s;
-    if (i < 0 || i >= T) return;
     const float *src = kFwd ? s.y : s.x;  // values of the other blocks
     int *fl = kFwd ? s.fy : s.fx;
     float acc0 = 0.f, acc1 = 0.f;
@@ -527,7 +519,11 @@ __global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
             }
         }
     }
-    if (!kFwd) load_slice(s, i, i, r2, cg, w);  // D_i, before the reduction
+    if (!kFwd) {
+        load_slice(s, i, i, r2, cg, w);  // D_i, before the reduction
+        // y_i comes from the forward pass of this launch
+        if (tid == 0 && !wait_flag(&s.fy[i], s.epoch, s.flags)) gave_up(s.flags);
+    }
     red[cg][2 * r2] = acc0;
     red[cg][2 * r2 + 1] = acc1;
     __syncthreads();
@@ -537,7 +533,7 @@ __global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
         if (kFwd)
             base = gr < s.n ? (float)s.b[gr] : 0.f;
         else
-            base = s.y[gr];
+            base = __ldcg(s.y + gr);
         const float z = base - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
         if (kFwd)
             s.y[gr] = z;
@@ -563,6 +559,24 @@ __global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
     __threadfence();
     __syncthreads();
     if (tid == 0) st_rel(&fl[i], s.epoch);
+}
+
+// Both passes in one launch of 2T CTAs: tickets 0..T-1 are the forward pass's
+// blocks 0..T-1, tickets T..2T-1 the backward pass's blocks T-1..0, so every
+// wait (forward: lower blocks; backward: higher blocks and its own forward
+// block) is on a lower ticket, held by a CTA that is already running.
+__global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
+    __shared__ int tk_s;
+    __shared__ float red[4][kB];
+    __shared__ float zs[kB];
+    const int T = s.T;
+    if (threadIdx.x == 0) tk_s = atomicAdd(&s.ticket[0], 1);
+    __syncthreads();
+    const int t = tk_s;
+    if (t < T)
+        solve_block<true>(s, t, red, zs);
+    else if (t < 2 * T)
+        solve_block<false>(s, 2 * T - 1 - t, red, zs);
 }
 
 // Self-test of the bounded waits: the cooperative LU's grid barrier with a CTA
@@ -676,11 +690,9 @@ void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, 
     s.ticket = B.ticket + 1;
     s.epoch = ++B.state->solve_epoch;
     s.flags = flags;
-    D4_CUDA_OK(cudaMemsetAsync(B.ticket + 1, 0, 2 * sizeof(int), st));
-    blu::k_bsolve32<true><<<T, blu::kThreads, 0, st>>>(s);
-    check_launch("k_bsolve32<fwd>");
-    blu::k_bsolve32<false><<<T, blu::kThreads, 0, st>>>(s);
-    check_launch("k_bsolve32<bwd>");
+    D4_CUDA_OK(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), st));
+    blu::k_bsolve32<<<2 * T, blu::kThreads, 0, st>>>(s);
+    check_launch("k_bsolve32");
 }
 
 int wait_selftest(int which) {

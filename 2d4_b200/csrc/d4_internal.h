@@ -315,6 +315,9 @@ void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const do
                    const double *y, double ext, double *v);
 int factor32(Ctx &c);
 int coop_grid_size32(int n);
+// The mixed form's field at points: FP64 stress, FP32 gradient.
+void field_eval_mixed(Ctx &c, int count, const double *dx, const double *dy, double *xy,
+                      double *xyd);
 
 // ---- mixed form's block LU (d4_blu32.cu) ----
 constexpr double kRefineLimit = 1e-9;  // refined max|r| / max|g| above this: exact path

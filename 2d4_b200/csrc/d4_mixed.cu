@@ -272,9 +272,28 @@ __global__ void k_ir_apply(int n, const double *dx, const int *flags, const doub
     out[i] = base[i] - d;
 }
 
+// The mixed form's field at single points: the FP64 stress its speeds use and
+// the FP32 gradient its matrix uses (the same calls as k_pairs32).
+__global__ void k_field_mixed(int count, const double *dx, const double *dy, double *xy,
+                              double *xyd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const double x = dx[k], y = dy[k];
+    xy[k] = f64::xy(x, y, f64::Hyp(f64::exp2pix(x)), f64::cos2piy(y));
+    float s, sd;
+    f32::field<true>((float)x, (float)y, s, sd);
+    xyd[k] = (double)sd;
+}
+
 inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
+
+void field_eval_mixed(Ctx &c, int count, const double *dx, const double *dy, double *xy,
+                      double *xyd) {
+    k_field_mixed<<<nb(count, 128), 128, 0, c.stream>>>(count, dx, dy, xy, xyd);
+    check_launch("k_field_mixed");
+}
 
 static Pair32Args pair32(Ctx &c, const double *x, const double *y) {
     Pair32Args a;

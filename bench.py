@@ -512,14 +512,16 @@ def ensemble_leg(pkg, count=512, rounds=3, seed=2000):
             "attempted_dislocation_steps_per_s": att / dev}
 
 
-def adjoint_leg(pkg, n=2048, steps=200, seed=1003, tau=0.08, k=20, fd_coords=4):
+def adjoint_leg(pkg, n=2048, steps=200, seed=1003, tau=0.08, k=20, fd_coords=32):
     """The adjoint workload: N=2048 (seed 1003), tau_ext = 0.08, 200 accepted
     steps recorded from the adaptive run; d strain / d (x0, tau0) by the
     adjoint with checkpoints every 20 steps; checked against the FP64
     tangent-linear along a random direction and against central differences
-    (h = 1e-6) on `fd_coords` coordinates drawn with seed 4000 (a coordinate
-    whose one-sided quotients disagree by more than 1e-4 is not converged at
-    that h and is reported separately)."""
+    (h = 1e-6) on `fd_coords` coordinates drawn with seed 4000.  A coordinate
+    whose one-sided quotients disagree by more than 1e-4 relative has no
+    converged central quotient at that h (a dipole closing within ~1e-5); for
+    those the quotient is redone at h = 1e-7 and 1e-8 and the best agreement
+    is reported separately."""
     x, y, _ = pkg.dconf.generate_internal(n, seed)
     sd = pkg.SimulationData()
     sd.set_positions(x, y)
@@ -537,23 +539,33 @@ def adjoint_leg(pkg, n=2048, steps=200, seed=1003, tau=0.08, k=20, fd_coords=4):
     rng = np.random.default_rng(4000)
     d = rng.standard_normal(n)
     _, ds = e.tangent(x, t0s, hs, d, 0.0)
-    h = 1e-6
-    fd, unconv = [], []
-    for i in rng.choice(n, fd_coords, replace=False):
+
+    def central(i, h):
         xp, xm = x.copy(), x.copy()
         xp[i] += h
         xm[i] -= h
         sp, sm = e.replay(xp, t0s, hs)[0], e.replay(xm, t0s, hs)[0]
-        q, qp, qm = (sp - sm) / (2 * h), (sp - s0) / h, (s0 - sm) / h
+        return (sp - sm) / (2 * h), (sp - s0) / h, (s0 - sm) / h
+
+    fd, unconv, sweep = [], [], []
+    for i in rng.choice(n, fd_coords, replace=False):
+        q, qp, qm = central(i, 1e-6)
         rel = abs(q - g[i]) / abs(g[i])
-        (fd if abs(qp - qm) <= 1e-4 * abs(q) else unconv).append(rel)
+        if abs(qp - qm) <= 1e-4 * abs(q):
+            fd.append(rel)
+        else:
+            unconv.append(int(i))
+            best = min(abs(central(i, h)[0] - g[i]) / abs(g[i]) for h in (1e-7, 1e-8))
+            sweep.append(best)
     e.close()
     return {"n": n, "steps": int(len(t0s)), "checkpoint_every": k, "strain": s,
             "replay_seconds": t_rep, "adjoint_seconds": t_adj,
             "adjoint_dislocation_steps_per_s": n * len(t0s) / t_adj,
             "grad_tau0": gt, "tangent_linear_rel_diff": abs(ds - g @ d) / abs(ds),
-            "fd_h": h, "fd_coords": fd_coords, "fd_max_rel_err": max(fd) if fd else None,
-            "fd_unconverged_coords": len(unconv)}
+            "fd_h": 1e-6, "fd_coords": fd_coords, "fd_converged_coords": len(fd),
+            "fd_max_rel_err": max(fd) if fd else None,
+            "fd_unconverged_coords": unconv,
+            "fd_unconverged_best_rel_err_h_1e-7_or_1e-8": sweep}
 
 
 def run_reference_arm(args, wl):

@@ -389,7 +389,9 @@ int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress
                       double *tol, double min_prec_sq, void *stream);
 
 /* Single field evaluations on the device, for checks: the context's field
- * (analytic FP64 Field::xy / Field::xy_diff_x, or the tabulated field). */
+ * (analytic FP64 Field::xy / Field::xy_diff_x, or the tabulated field; in the
+ * mixed form the FP64 stress its speeds use and the FP32 compensated gradient
+ * its matrix uses). */
 int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
                   double *xy_diff_x);
 

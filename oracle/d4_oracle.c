@@ -189,6 +189,130 @@ double d4o_xy_diff_x(double dx, double dy) {
     return d4o_xy_diff_x4(dx, dy, e, c);
 }
 
+/* ------------------------------------------- IEEE variant of the field -- */
+/* The reference's exact truncated image sum with cosh and sinh, compiled when
+ * USE_IEEE_HYPERBOLIC is 1 (src/Fields/Field.cpp:26-168; the same expressions
+ * as sandbox/ieee_hyperbolic/ieee_hyperbolic.cpp:11-140, which the tests
+ * build as the pin).  Not on the reference's default path: the secondary
+ * oracle of the field, against which the FP32 gradient's error is measured.
+ * Every expression keeps the reference's operation order (pow for the integer
+ * powers, as std::pow(double, int) does). */
+
+/* f, src/Fields/Field.cpp:28-44: one wall image. */
+static double ieee_f(double dx, double cos2piy, double dy) {
+    if (dx * dx + dy * dy > 1e-6) {
+        double cosh2pix = cosh(dx * 2 * M_PI);
+        double coshpixyd = cosh2pix - cos2piy;
+        return dx * (cosh2pix * cos2piy - 1) / pow(coshpixyd, 2) * 2 * M_PI * M_PI;
+    }
+    double dx2pi = dx * 2 * M_PI;
+    double dy2pi = dy * 2 * M_PI;
+    double cosh2pixminus1 = pow(dx2pi, 6) / 720 + pow(dx2pi, 4) / 24 + pow(dx2pi, 2) * 0.5;
+    double cos2piyminus1 = -pow(dy2pi, 6) / 720 + pow(dy2pi, 4) / 24 - pow(dy2pi, 2) * 0.5;
+    double coshminuscos = (pow(dy2pi, 6) + pow(dx2pi, 6)) / 720 +
+                          (pow(dx2pi, 4) - pow(dy2pi, 4)) / 24 +
+                          (pow(dx2pi, 2) + pow(dy2pi, 2)) * 0.5;
+    return ((cosh2pixminus1 * cos2piyminus1 + cos2piyminus1 + cosh2pixminus1) * dx) /
+           pow(coshminuscos, 2) * 2 * M_PI * M_PI;
+}
+
+/* g<images>, src/Fields/Field.cpp:47-58: g<0> = f(dx), then
+ * g<k> = g<k-1> + f(dx - k) + f(dx + k). */
+static double ieee_g(int images, double dx, double cos2piy, double dy) {
+    double s = ieee_f(dx, cos2piy, dy);
+    for (int k = 1; k <= images; ++k) {
+        s = s + ieee_f(dx - k, cos2piy, dy);
+        s = s + ieee_f(dx + k, cos2piy, dy);
+    }
+    return s;
+}
+
+/* f_dx, src/Fields/Field.cpp:61-105: x-derivative of one wall image. */
+static double ieee_f_dx(double dx, double cos2piy, double dy) {
+    double dx2pi = dx * 2 * M_PI;
+    if (dx * dx + dy * dy > 1e-6) {
+        double cosh2pix = cosh(dx2pi);
+        double sinh2pix = sinh(dx2pi);
+        double coshpixyd = cosh2pix - cos2piy;
+        return ((cosh2pix * cos2piy - 1) / pow(coshpixyd, 2) +
+                dx * (sinh2pix * cos2piy * 2 * M_PI / pow(coshpixyd, 2) -
+                      (cosh2pix * cos2piy - 1) / pow(coshpixyd, 3) * 4 * M_PI * sinh2pix)) *
+               M_PI * 2 * M_PI;
+    }
+    double dy2pi = dy * M_PI * 2;
+    double cosh2pixminus1 = pow(dx2pi, 6) / 720 + pow(dx2pi, 4) / 24 + pow(dx2pi, 2) * 0.5;
+    double cos2piyminus1 = -pow(dy2pi, 6) / 720 + pow(dy2pi, 4) / 24 - pow(dy2pi, 2) * 0.5;
+    double coshminuscos = (pow(dy2pi, 6) + pow(dx2pi, 6)) / 720 +
+                          (pow(dx2pi, 4) - pow(dy2pi, 4)) / 24 +
+                          (pow(dx2pi, 2) + pow(dy2pi, 2)) * 0.5;
+    double cosysinhx = -(pow(dx2pi, 7) * pow(dy2pi, 6)) / 3628800
+                       - (pow(dx2pi, 5) * pow(dy2pi, 6)) / 86400
+                       - (pow(dx2pi, 3) * pow(dy2pi, 6)) / 4320
+                       - (pow(dy2pi, 6) * dx2pi) / 720
+                       + (pow(dx2pi, 7) * pow(dy2pi, 4)) / 120960
+                       + (pow(dx2pi, 5) * pow(dy2pi, 4)) / 2880
+                       + (pow(dx2pi, 3) * pow(dy2pi, 4)) / 144
+                       + (pow(dy2pi, 4) * dx2pi) / 24
+                       - (pow(dx2pi, 7) * pow(dy2pi, 2)) / 1080
+                       - (pow(dx2pi, 5) * pow(dy2pi, 2)) / 240
+                       - (pow(dx2pi, 3) * pow(dy2pi, 2)) / 12
+                       - (pow(dy2pi, 2) * dx2pi) * 0.5
+                       + pow(dx2pi, 7) / 5040
+                       + pow(dx2pi, 5) / 120
+                       + pow(dx2pi, 3) / 6
+                       + dx2pi;
+    return ((cosh2pixminus1 * cos2piyminus1 + cos2piyminus1 + cosh2pixminus1) /
+                pow(coshminuscos, 2) +
+            ((cosysinhx * dx) / pow(coshminuscos, 2) -
+             (cosh2pixminus1 * cos2piyminus1 + cos2piyminus1 + cosh2pixminus1) /
+                 pow(coshminuscos, 3) * dx * sinh(dx2pi) * 2) *
+                2 * M_PI) *
+           M_PI * 2 * M_PI;
+}
+
+/* g_dx<images>, src/Fields/Field.cpp:108-119. */
+static double ieee_g_dx(int images, double dx, double cos2piy, double dy) {
+    double s = ieee_f_dx(dx, cos2piy, dy);
+    for (int k = 1; k <= images; ++k) {
+        s = s + ieee_f_dx(dx - k, cos2piy, dy);
+        s = s + ieee_f_dx(dx + k, cos2piy, dy);
+    }
+    return s;
+}
+
+#define D4O_FIELD_N 4 /* ANALYTIC_FIELD_N, include/constants.h */
+
+/* Field::xy (IEEE), src/Fields/Field.cpp:122-137. */
+double d4o_ieee_xy(double dx, double dy) {
+    double cos2piy = cos(M_PI * 2 * dy);
+    if (dx < 0)
+        return -dx * ieee_f(dx + D4O_FIELD_N + 1, cos2piy, dy) +
+               (1 + dx) * ieee_f(dx - D4O_FIELD_N, cos2piy, dy) +
+               ieee_f(dx + D4O_FIELD_N, cos2piy, dy) +
+               ieee_g(D4O_FIELD_N - 1, dx, cos2piy, dy);
+    return dx * ieee_f(dx - D4O_FIELD_N - 1, cos2piy, dy) +
+           (1 - dx) * ieee_f(dx + D4O_FIELD_N, cos2piy, dy) +
+           ieee_f(dx - D4O_FIELD_N, cos2piy, dy) + ieee_g(D4O_FIELD_N - 1, dx, cos2piy, dy);
+}
+
+/* Field::xy_diff_x (IEEE), src/Fields/Field.cpp:146-164. */
+double d4o_ieee_xy_diff_x(double dx, double dy) {
+    double cos2piy = cos(M_PI * 2 * dy);
+    if (dx < 0)
+        return -ieee_f(dx + D4O_FIELD_N + 1, cos2piy, dy) -
+               dx * ieee_f_dx(dx + D4O_FIELD_N + 1, cos2piy, dy) +
+               ieee_f_dx(dx - D4O_FIELD_N, cos2piy, dy) * (1 + dx) +
+               ieee_f(dx - D4O_FIELD_N, cos2piy, dy) +
+               ieee_f_dx(dx + D4O_FIELD_N, cos2piy, dy) +
+               ieee_g_dx(D4O_FIELD_N - 1, dx, cos2piy, dy);
+    return ieee_f(dx - D4O_FIELD_N - 1, cos2piy, dy) +
+           dx * ieee_f_dx(dx - D4O_FIELD_N - 1, cos2piy, dy) +
+           ieee_f_dx(dx + D4O_FIELD_N, cos2piy, dy) * (1 - dx) -
+           ieee_f(dx + D4O_FIELD_N, cos2piy, dy) +
+           ieee_f_dx(dx - D4O_FIELD_N, cos2piy, dy) +
+           ieee_g_dx(D4O_FIELD_N - 1, dx, cos2piy, dy);
+}
+
 /* ------------------------------------------------------------ utilities -- */
 
 /* normalize, src/sim_utils.cpp:6-13. */

@@ -77,6 +77,9 @@ double d4o_xy(double dx, double dy);
 double d4o_xy_diff_x(double dx, double dy);
 double d4o_xy4(double dx, double dy, double exp2pix, double cos2piy);
 double d4o_xy_diff_x4(double dx, double dy, double exp2pix, double cos2piy);
+/* The IEEE variant (USE_IEEE_HYPERBOLIC 1), src/Fields/Field.cpp:26-168. */
+double d4o_ieee_xy(double dx, double dy);
+double d4o_ieee_xy_diff_x(double dx, double dy);
 
 double d4o_normalize(double v);
 double d4o_weight(double s, char t);

@@ -86,6 +86,9 @@ class Restated:
         for f in ("d4o_xy", "d4o_xy_diff_x", "d4o_xy4", "d4o_xy_diff_x4", "d4o_normalize",
                   "d4o_weight", "d4o_weight_inv", "d4o_ext_stress"):
             getattr(L, f).restype = C.c_double
+        for f in ("d4o_ieee_xy", "d4o_ieee_xy_diff_x"):
+            getattr(L, f).restype = C.c_double
+            getattr(L, f).argtypes = [C.c_double, C.c_double]
         for f in ("d4o_xy", "d4o_xy_diff_x"):
             getattr(L, f).argtypes = [C.c_double, C.c_double]
         for f in ("d4o_xy4", "d4o_xy_diff_x4"):

@@ -21,7 +21,11 @@ unmodified, -O2 -ffp-contract=off, with the project's UMFPACK shim):
          src/simulation.cpp:232-247, simulation_data.cpp:231-246) by file name;
   aval_* the same fixture at zero stress, P = 1e-8, stopped by the avalanche
          detection limit 0 with speed threshold 0.05 (src/simulation.cpp:215-230,
-         722-750): final positions, counts and simulation time.
+         722-750): final positions, counts and simulation time;
+  ieee_* the IEEE variant of the field (src/Fields/Field.cpp:26-168) on the
+         field grid of golden.npz, from the reference's own IEEE evaluator
+         (sandbox/ieee_hyperbolic/ieee_hyperbolic.cpp:103-140, built in place
+         as oracle/_ref/libd4ref_ieee.so).
 Each case runs in its own process (the shim picks its LU backend at load).
 """
 import glob
@@ -104,6 +108,19 @@ def case(name):
         out["log_sub_names"] = np.array(names)
         for k, nm in enumerate(names):
             out["log_sub_%d" % k] = np.loadtxt(prefix + nm, ndmin=2)
+    elif name == "ieee":
+        import ctypes as C
+        L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libd4ref_ieee.so"))
+        for f in ("d4ref_ieee_xy", "d4ref_ieee_xy_diff_x"):
+            getattr(L, f).restype = C.c_double
+            getattr(L, f).argtypes = [C.c_double, C.c_double]
+        g = np.load(os.path.join(HERE, "golden.npz"))
+        fx, fy = g["field_dx"], g["field_dy"]
+        out["ieee_xy"] = np.array([L.d4ref_ieee_xy(a, b) for a, b in zip(fx, fy)])
+        out["ieee_xyd"] = np.array([L.d4ref_ieee_xy_diff_x(a, b) for a, b in zip(fx, fy)])
+        tmpnpz = os.path.join(tmp, name + ".npz")
+        np.savez_compressed(tmpnpz, **out)
+        return tmpnpz
     elif name == "aval":
         path = os.path.join(reference_root(), "init_config_gen", "README_files", "1000_64.dconf")
         ref = pyoracle.Reference("exact")
@@ -122,7 +139,7 @@ def case(name):
 
 
 def main(argv):
-    names = argv or ["log", "aval", "c2", "c3"]
+    names = argv or ["log", "aval", "ieee", "c2", "c3"]
     merged = dict(np.load(OUT)) if os.path.exists(OUT) else {}
     for name in names:
         r = subprocess.run([sys.executable, os.path.abspath(__file__), "--case", name],

@@ -103,3 +103,40 @@ def test_unsupported_forms_rejected(pkg, setup):
         with pytest.raises(pkg._lib.D4Error):
             e.replay(x, setup["t0s"][:1], setup["hs"][:1])
         e.close()
+
+
+def test_adjoint_c5_size_vs_central_differences(pkg):
+    """The adjoint configuration's own size: N=2048 (seed 1003), tau = 0.08, a
+    20-step recorded sequence, checkpoints every 20 steps; central differences
+    (h = 1e-6) on 16 coordinates drawn with seed 4000 agree with the adjoint to
+    1e-5 relative where the one-sided quotients agree (converged at that h);
+    a coordinate whose quotient has not converged at 1e-6 must meet the bound
+    at h = 1e-7 or 1e-8."""
+    n = 2048
+    x, y, _ = pkg.dconf.generate_internal(n, 1003)
+    sd = pkg.SimulationData()
+    sd.set_positions(x, y)
+    sd.external_stress = pkg.FixedRateProtocol(TAU, 0.0)
+    e = pkg.Engine(sd)
+    e.record_steps(True)
+    e.advance(20)
+    t0s, hs = e.recorded_steps()
+    s0, _ = e.replay(x, t0s, hs)
+    _, g, _ = e.adjoint(x, t0s, hs, checkpoint_every=20)
+
+    def central(i, h):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += h
+        xm[i] -= h
+        sp, sm = e.replay(xp, t0s, hs)[0], e.replay(xm, t0s, hs)[0]
+        return (sp - sm) / (2 * h), (sp - s0) / h, (s0 - sm) / h
+
+    rng = np.random.default_rng(4000)
+    for i in rng.choice(n, 16, replace=False):
+        q, qp, qm = central(i, 1e-6)
+        if abs(qp - qm) <= 1e-4 * abs(q):
+            assert abs(q - g[i]) <= 1e-5 * abs(g[i]), (i, q, g[i])
+        else:
+            best = min(abs(central(i, h)[0] - g[i]) for h in (1e-7, 1e-8))
+            assert best <= 1e-5 * abs(g[i]), (i, best, g[i])
+    e.close()
