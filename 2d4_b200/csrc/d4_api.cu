@@ -117,7 +117,7 @@ void free_all(Ctx *c) {
                     c->rowsub, c->rowsc,
                     c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
                     c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
-                    c->m_w1, c->m_resid, c->m_part, c->m_pp};
+                    c->m_w1, c->m_resid, c->m_part, c->m_pp, c->m_dx2, c->m_cnt};
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
@@ -128,7 +128,8 @@ void free_all(Ctx *c) {
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
                   c->xw2_b, c->dx_b, B.A32, B.LU32, B.P0, B.Q, B.mask, B.bar, B.perm, B.piv,
-                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, c->m_vacc_b, c->m_pp_b};
+                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, c->m_vacc_b, c->m_pp_b,
+                  B.dx2, B.cnt};
     for (void *b : ob)
         if (b) cudaFree(b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -764,8 +765,10 @@ int d4_create(void **out, int n, const d4_params *p) {
             dalloc(&c->LU32, nn);
             dalloc(&c->lu32_p0, (size_t)n * 32);
             dalloc(&c->lu32_q, (size_t)n * 64);
-            double **mv[] = {&c->m_vacc, &c->m_subacc, &c->m_g, &c->m_r, &c->m_dx};
+            double **mv[] = {&c->m_vacc, &c->m_subacc, &c->m_g, &c->m_r, &c->m_dx, &c->m_dx2};
             for (double **v : mv) dalloc(v, (size_t)n);
+            dalloc(&c->m_cnt, (size_t)(n + 255) / 256);
+            D4_CUDA_OK(cudaMemset(c->m_cnt, 0, sizeof(unsigned) * ((n + 255) / 256)));
             dalloc(&c->m_c32, (size_t)n);
             dalloc(&c->m_w1, (size_t)n);
             dalloc(&c->m_part, (size_t)((n + 255) / 256) * n);
@@ -846,6 +849,9 @@ int d4_create(void **out, int n, const d4_params *p) {
                 dalloc(&B.g, (size_t)n);
                 dalloc(&B.r, (size_t)n);
                 dalloc(&B.dx, (size_t)n);
+                dalloc(&B.dx2, (size_t)n);
+                dalloc(&B.cnt, (size_t)(n + 255) / 256);
+                D4_CUDA_OK(cudaMemset(B.cnt, 0, sizeof(unsigned) * ((n + 255) / 256)));
                 dalloc(&B.part, (size_t)((n + 255) / 256) * n);
                 dalloc(&B.c32, (size_t)n);
                 dalloc(&B.w1, (size_t)n);

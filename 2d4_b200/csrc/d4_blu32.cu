@@ -472,7 +472,7 @@ struct SolveArgs {
     const double *b;   // right-hand side (n)
     float *y, *x;      // T*128 each; x is the solution
     int *fy, *fx;      // T flags each (== epoch: block done)
-    int *ticket;       // ticket counter (zeroed before the launch)
+    int *ticket;       // ticket counter (0 at the launch; the CTA taking the last ticket resets it)
     int epoch;
     int *flags;        // kFlagBarrierTimeout
 };
@@ -570,7 +570,11 @@ __global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
     __shared__ float red[4][kB];
     __shared__ float zs[kB];
     const int T = s.T;
-    if (threadIdx.x == 0) tk_s = atomicAdd(&s.ticket[0], 1);
+    if (threadIdx.x == 0) {
+        const int t = atomicAdd(&s.ticket[0], 1);
+        if (t == 2 * T - 1) atomicExch(&s.ticket[0], 0);  // the last ticket: ready for the next launch
+        tk_s = t;
+    }
     __syncthreads();
     const int t = tk_s;
     if (t < T)
@@ -690,7 +694,6 @@ void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, 
     s.ticket = B.ticket + 1;
     s.epoch = ++B.state->solve_epoch;
     s.flags = flags;
-    D4_CUDA_OK(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), st));
     blu::k_bsolve32<<<2 * T, blu::kThreads, 0, st>>>(s);
     check_launch("k_bsolve32");
 }

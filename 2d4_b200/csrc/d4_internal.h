@@ -65,8 +65,9 @@ struct Mix32Bufs {
     float *A32 = nullptr, *LU32 = nullptr, *P0 = nullptr, *Q = nullptr;
     unsigned *mask = nullptr, *bar = nullptr;
     int *flags = nullptr, *perm = nullptr, *piv = nullptr;
-    double *g = nullptr, *r = nullptr, *dx = nullptr;
+    double *g = nullptr, *r = nullptr, *dx = nullptr, *dx2 = nullptr;
     double *part = nullptr;  // ceil(n / 256) x n: the residual product's column-chunk sums
+    unsigned *cnt = nullptr; // ceil(n / 256): chunk blocks finished per row block (k_resid_fused)
     float *c32 = nullptr, *w1 = nullptr;
     unsigned long long *resid = nullptr;  // 8 pairs (max |r|, max |g|)
     int *resid_count = nullptr;           // host: next slot of resid
@@ -151,7 +152,8 @@ struct Ctx {
     float *A32 = nullptr, *LU32 = nullptr, *lu32_p0 = nullptr, *lu32_q = nullptr;
     int lu32_grid = 0;
     double *m_vacc = nullptr, *m_subacc = nullptr, *m_g = nullptr, *m_r = nullptr,
-           *m_dx = nullptr;
+           *m_dx = nullptr, *m_dx2 = nullptr;
+    unsigned *m_cnt = nullptr;
     float *m_c32 = nullptr, *m_w1 = nullptr;
     double *m_part = nullptr;  // residual product's column-chunk sums (Mix32Bufs::part)
     double *m_pp = nullptr, *m_pp_b = nullptr;  // pair-tile row partials, 4 x ceil(n/32) x n

@@ -13,6 +13,7 @@
 //     dx = 0, r = g;  repeat: c = LU32 \ r;  dx += c;  r = g - A32 dx
 // so the solution of A32 dx = g is accurate to FP64 rounding times cond(A).
 #include <cstdint>
+#include <utility>
 
 #include "d4_field32.cuh"
 #include "d4_field64.cuh"
@@ -214,34 +215,47 @@ __global__ void k_ir_init(int n, trsv::GArgs ga, double *g, double *r, double *d
     dx[i] = 0;
 }
 
-// dx += c (float correction); r is then recomputed from g by k_resid32.
-__global__ void k_ir_accum(int n, const float *c, double *dx) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    dx[i] += (double)c[i];
-}
-
-// (A32 dx)_i over a chunk of columns per block (FP64 accumulation), into
-// part[chunk][i].
-__global__ void __launch_bounds__(256) k_gemv_part32(int n, const float *__restrict__ A,
-                                                     const double *__restrict__ dx, double *part,
-                                                     int chunk) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One refinement update in one launch: dx_out = dx + c and r = g - A32 dx_out.
+// Block (x, y) multiplies rows 256x.. by column chunk y (FP64 accumulation in
+// column order, the chunk's corrected dx staged in shared memory; the blocks of
+// row block 0 also store it to dx_out, a buffer no block reads) into
+// part[y][i]; the last block of each row block to finish (a counter per row
+// block, reset by that block) subtracts the chunk sums from g in chunk order.
+// The arithmetic and its order are those of a separate update, product and
+// residual, so the residual is the same on every run.
+__global__ void __launch_bounds__(256) k_resid_fused(int n, const float *__restrict__ A,
+                                                     const double *__restrict__ dx,
+                                                     const float *__restrict__ corr,
+                                                     double *dx_out, const double *g,
+                                                     double *part, int chunk, int nch,
+                                                     unsigned *cnt, double *r) {
+    __shared__ double sdx[256];
+    __shared__ int last;
     const int c0 = blockIdx.y * chunk, c1 = min(n, c0 + chunk);
-    if (i >= n) return;
-    double s = 0;
-    for (int c = c0; c < c1; ++c) s += (double)__ldg(A + (size_t)i + (size_t)c * n) * dx[c];
-    part[(size_t)blockIdx.y * n + i] = s;
-}
-
-// r = g - A32 dx: the chunk sums subtracted in chunk order, so the residual,
-// and every correction computed from it, is the same on every run.
-__global__ void k_resid32(int n, const double *g, const double *part, int nch, double *r) {
+    for (int t = threadIdx.x; t < c1 - c0; t += blockDim.x) {
+        const double v = dx[c0 + t] + (double)corr[c0 + t];
+        sdx[t] = v;
+        if (blockIdx.x == 0) dx_out[c0 + t] = v;
+    }
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double v = g[i];
-    for (int q = 0; q < nch; ++q) v = v - part[(size_t)q * n + i];
-    r[i] = v;
+    if (i < n) {
+        double s = 0;
+        for (int c = c0; c < c1; ++c) s += (double)__ldg(A + (size_t)i + (size_t)c * n) * sdx[c - c0];
+        part[(size_t)blockIdx.y * n + i] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&cnt[blockIdx.x], 1u) == (unsigned)(nch - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (i < n) {
+        double v = g[i];
+        for (int q = 0; q < nch; ++q) v = v - __ldcg(part + (size_t)q * n + i);
+        r[i] = v;
+    }
+    if (threadIdx.x == 0) cnt[blockIdx.x] = 0;
 }
 
 // max |r| and max |g| into out[0], out[1] (as ordered bits of non-negatives).
@@ -375,6 +389,8 @@ Mix32Bufs primary_mix32(Ctx &c) {
     B.g = c.m_g;
     B.r = c.m_r;
     B.dx = c.m_dx;
+    B.dx2 = c.m_dx2;
+    B.cnt = c.m_cnt;
     B.part = c.m_part;
     B.c32 = c.m_c32;
     B.w1 = c.m_w1;
@@ -479,6 +495,22 @@ static const float *solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, co
     return B.c32;
 }
 
+// The refinement loop: c = LU32^-1 r, dx += c, r = g - A32 dx, c.ir_iters
+// times from dx = 0, r = g (k_ir_init); dx alternates between B.dx and B.dx2.
+// Returns the buffer holding the final dx.
+static const double *refine(Ctx &c, const Mix32Bufs &B, cudaStream_t st) {
+    const int n = c.n, chunk = 256;
+    double *dxa = B.dx, *dxb = B.dx2;
+    for (int it = 0; it < c.ir_iters; ++it) {
+        const float *corr = solve32_once(c, B, st, B.r);
+        k_resid_fused<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(
+            n, B.A32, dxa, corr, dxb, B.g, B.part, chunk, nb(n, chunk), B.cnt, B.r);
+        check_launch("k_resid_fused");
+        std::swap(dxa, dxb);
+    }
+    return dxa;
+}
+
 void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
                          cudaStream_t st, int gmode, double hval, const double *s_end,
                          const double *s_init, const double *x_new, const double *x_old,
@@ -494,21 +526,11 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
     ga.x_old = x_old;
     k_ir_init<<<nb(n, 256), 256, 0, st>>>(n, ga, B.g, B.r, B.dx);
     check_launch("k_ir_init");
-    const int chunk = 256;
-    for (int it = 0; it < c.ir_iters; ++it) {
-        const float *corr = solve32_once(c, B, st, B.r);
-        k_ir_accum<<<nb(n, 256), 256, 0, st>>>(n, corr, B.dx);
-        check_launch("k_ir_accum");
-        k_gemv_part32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(n, B.A32, B.dx, B.part,
-                                                                      chunk);
-        check_launch("k_gemv_part32");
-        k_resid32<<<nb(n, 256), 256, 0, st>>>(n, B.g, B.part, nb(n, chunk), B.r);
-        check_launch("k_resid32");
-    }
+    const double *dx = refine(c, B, st);
     k_absmax2<<<64, 256, 0, st>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");
     *B.resid_count = (*B.resid_count + 1) % 8;
-    k_ir_apply<<<nb(n, 256), 256, 0, st>>>(n, B.dx, B.flags, base, out, dx_out);
+    k_ir_apply<<<nb(n, 256), 256, 0, st>>>(n, dx, B.flags, base, out, dx_out);
     check_launch("k_ir_apply");
 }
 
@@ -520,21 +542,11 @@ void solve_plain32(Ctx &c, const double *g) {
     ga.g_in = g;
     k_ir_init<<<nb(n, 256), 256, 0, c.stream>>>(n, ga, B.g, B.r, B.dx);
     check_launch("k_ir_init");
-    const int chunk = 256;
-    for (int it = 0; it < c.ir_iters; ++it) {
-        const float *corr = solve32_once(c, B, c.stream, B.r);
-        k_ir_accum<<<nb(n, 256), 256, 0, c.stream>>>(n, corr, B.dx);
-        check_launch("k_ir_accum");
-        k_gemv_part32<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, c.stream>>>(n, B.A32, B.dx,
-                                                                             B.part, chunk);
-        check_launch("k_gemv_part32");
-        k_resid32<<<nb(n, 256), 256, 0, c.stream>>>(n, B.g, B.part, nb(n, chunk), B.r);
-        check_launch("k_resid32");
-    }
+    const double *dx = refine(c, B, c.stream);
     k_absmax2<<<64, 256, 0, c.stream>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");
     *B.resid_count = (*B.resid_count + 1) % 8;
-    D4_CUDA_OK(cudaMemcpyAsync(c.dx, B.dx, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+    D4_CUDA_OK(cudaMemcpyAsync(c.dx, dx, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                                c.stream));
 }
 
