@@ -116,8 +116,8 @@ void free_all(Ctx *c) {
                     c->wave_err, c->xw1, c->xw2,
                     c->rowsub, c->rowsc,
                     c->lu_p0, c->lu_q, c->lu_mask, c->lu_bar, c->A32, c->LU32, c->lu32_p0,
-                    c->lu32_q, c->m_vacc, c->m_subacc, c->m_g, c->m_r, c->m_dx, c->m_c32,
-                    c->m_w1, c->m_resid, c->m_part, c->m_pp, c->m_dx2, c->m_cnt};
+                    c->lu32_q, c->m_g, c->m_r, c->m_dx, c->m_c32, c->m_w1, c->m_resid,
+                    c->m_part, c->m_dx2, c->m_cnt, c->m_conv, c->spiv};
     for (void *b : bufs)
         if (b) cudaFree(b);
     d4::sparse_free(*c);
@@ -128,8 +128,7 @@ void free_all(Ctx *c) {
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
                   c->xw2_b, c->dx_b, B.A32, B.LU32, B.P0, B.Q, B.mask, B.bar, B.perm, B.piv,
-                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, c->m_vacc_b, c->m_pp_b,
-                  B.dx2, B.cnt};
+                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, B.dx2, B.cnt, B.conv, B.A64};
     for (void *b : ob)
         if (b) cudaFree(b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -350,12 +349,13 @@ static double worst_refined(const unsigned long long *rb) {
 }
 
 // The mixed form's stages I-IV with stage I on a second stream, as
-// attempt_overlap: stage I copies A1 into its own FP32 matrix (the one its
-// refinement multiplies) while factorising it, and runs its two refined solves
-// and its stress sweep on stream_b with its own buffers; stages II and III run
-// on the context's stream.  Every operation is the sequential attempt's, so
-// the results are identical.  *refine_out: the worst refined residual of the
-// attempt's six solves.
+// attempt_overlap: the FP64 form's sweeps and rescale, the factorisations and
+// refined solves of d4_mixed.cu.  Stage I copies A1 into its own FP64 matrix
+// (the one its refinement multiplies) before factorising it, and runs its two
+// solves and its stress sweep on stream_b with its own buffers; stages II and
+// III run on the context's stream.  Every operation is the sequential
+// attempt's, so the results are identical.  *refine_out: the worst refined
+// residual of the attempt's six solves.
 static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out,
                                   double *refine_out) {
     using d4::ProfScope;
@@ -371,7 +371,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     cudaStream_t sa = c.stream, sb = c.stream_b;
     {
         ProfScope ps(c, D4_CAT_JACOBIAN);
-        d4::jacobian32(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t1), c.v_init, c.speed);
+        d4::jacobian64(c, c.x0, c.y, h, ext_stress(pr, t0), ext_stress(pr, t1), c.v_init, c.speed);
     }
     D4_CUDA_OK(cudaMemcpyAsync(c.dvec_b, c.dvec, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
     D4_CUDA_OK(cudaMemcpyAsync(c.speed_b, c.speed, sizeof(double) * n, cudaMemcpyDeviceToDevice, sa));
@@ -380,7 +380,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     // stage I on stream_b
     {
         ProfScope ps(c, D4_CAT_FACTOR, sb);
-        d4::factor32_async(c, B1, c.A32, true, g1, sb, c.ev_copy);
+        d4::factor32_async(c, B1, c.A, true, g1, sb, c.ev_copy);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE, sb);
@@ -389,7 +389,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     }
     {
         ProfScope ps(c, D4_CAT_SPEEDS, sb);
-        d4::speeds32_with(c, c.m_vacc_b, c.m_pp_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
+        d4::speeds64_with(c, c.F_b, sb, c.xb, c.y, ext_stress(pr, t1), c.speed2_b);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE, sb);
@@ -401,11 +401,11 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     D4_CUDA_OK(cudaStreamWaitEvent(sa, c.ev_copy, 0));
     {
         ProfScope ps(c, D4_CAT_RESCALE);
-        d4::jacobian_from_prev32(c, (th - t0) / (t1 - t0));
+        d4::jacobian_from_prev64(c, (th - t0) / (t1 - t0));
     }
     {
         ProfScope ps(c, D4_CAT_FACTOR);
-        d4::factor32_async(c, B2, c.A32, false, g2, sa, nullptr);
+        d4::factor32_async(c, B2, c.A, false, g2, sa, nullptr);
     }
     d4::shift_speed64(c, c.speed, ext_stress(pr, th) - ext_stress(pr, t1));
     {
@@ -415,7 +415,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     }
     {
         ProfScope ps(c, D4_CAT_SPEEDS);
-        d4::speeds32(c, c.xh, c.y, ext_stress(pr, th), c.speed2);
+        d4::speeds64(c, c.xh, c.y, ext_stress(pr, th), c.speed2);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE);
@@ -425,12 +425,12 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     // stage III
     {
         ProfScope ps(c, D4_CAT_JACOBIAN);
-        d4::jacobian32(c, c.xh, c.y, h / 2, ext_stress(pr, th), ext_stress(pr, t1), c.v_init2,
+        d4::jacobian64(c, c.xh, c.y, h / 2, ext_stress(pr, th), ext_stress(pr, t1), c.v_init2,
                        c.speed2);
     }
     {
         ProfScope ps(c, D4_CAT_FACTOR);
-        d4::factor32_async(c, B3, c.A32, false, c.lu32_grid, sa, nullptr);
+        d4::factor32_async(c, B3, c.A, false, c.lu32_grid, sa, nullptr);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE);
@@ -439,7 +439,7 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
     }
     {
         ProfScope ps(c, D4_CAT_SPEEDS);
-        d4::speeds32(c, c.x2, c.y, ext_stress(pr, t1), c.speed2);
+        d4::speeds64(c, c.x2, c.y, ext_stress(pr, t1), c.speed2);
     }
     {
         ProfScope ps(c, D4_CAT_SOLVE);
@@ -503,10 +503,7 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
     const bool mixed = c.p.precision == D4_PREC_MIXED;
     auto jac = [&](const double *x, double hh, double ta, double tb, double *va, double *vb) {
         ProfScope ps(c, D4_CAT_JACOBIAN);
-        if (mixed)
-            d4::jacobian32(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
-        else
-            d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
+        d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
     };
     const bool gmres = c.use_gmres != 0;
     auto dense_fac = [&]() {
@@ -523,10 +520,7 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
     };
     auto spd = [&](const double *x, double t, double *v) {
         ProfScope ps(c, D4_CAT_SPEEDS);
-        if (mixed)
-            d4::speeds32(c, x, c.y, ext_stress(pr, t), v);
-        else
-            d4::speeds64(c, x, c.y, ext_stress(pr, t), v);
+        d4::speeds64(c, x, c.y, ext_stress(pr, t), v);
     };
     auto slv = [&](int gmode, double hv, const double *se, const double *si, const double *xn,
                    const double *xo, const double *base, double *out) {
@@ -554,10 +548,7 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
         const double factor = (t_1p2 - t0) / (t_1__ - t0);
         {
             ProfScope ps(c, D4_CAT_RESCALE);
-            if (mixed)
-                d4::jacobian_from_prev32(c, factor);
-            else
-                d4::jacobian_from_prev64(c, factor);
+            d4::jacobian_from_prev64(c, factor);
         }
         fac();
         const double dif = ext_stress(pr, t_1p2) - ext_stress(pr, t_1__);
@@ -620,31 +611,20 @@ int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
         throw;
     }
     c.m_fast = 1;
+    d4::adopt_pivots(c);  // the next block LUs factorise P A with this attempt's P
     return D4_OK;
 }
 
-// Stress sweep of the context's form (FP64 buffers exist only in the FP64 form).
+// Stress sweep (both forms use the FP64 sweeps).
 void sweep_speeds(Ctx &c, const double *x, const double *y, double ext, double *v) {
-    if (c.p.precision == D4_PREC_MIXED)
-        d4::speeds32(c, x, y, ext, v);
-    else
-        d4::speeds64(c, x, y, ext, v);
+    d4::speeds64(c, x, y, ext, v);
 }
 
-// Device matrix (FP64, or the mixed form's FP32 widened) to a host buffer.
+// Device matrix (FP64 in both forms) to a host buffer.
 void copy_matrix_out(Ctx &c, double *dst) {
     if (!dst) return;
     const size_t nn = (size_t)c.n * c.n;
-    if (c.p.precision == D4_PREC_MIXED) {
-        std::vector<float> tmp(nn);
-        D4_CUDA_OK(cudaMemcpyAsync(tmp.data(), c.A32, sizeof(float) * nn, cudaMemcpyDeviceToHost,
-                                   c.stream));
-        sync(c);
-        for (size_t k = 0; k < nn; ++k) dst[k] = tmp[k];
-    } else {
-        D4_CUDA_OK(cudaMemcpyAsync(dst, c.A, sizeof(double) * nn, cudaMemcpyDeviceToHost,
-                                   c.stream));
-    }
+    D4_CUDA_OK(cudaMemcpyAsync(dst, c.A, sizeof(double) * nn, cudaMemcpyDeviceToHost, c.stream));
 }
 
 double host_abs_sum(const std::vector<double> &v) {
@@ -757,25 +737,30 @@ int d4_create(void **out, int n, const d4_params *p) {
                            &c->dvec_new, &c->fac, &c->dx, &c->tol};
         for (double **v : vecs) dalloc(v, (size_t)n);
         const bool mixed = p->precision == D4_PREC_MIXED;
-        dalloc(&c->A, mixed ? 1 : nn);
+        // both forms: the FP64 matrix and pair-force scratch of the FP64 sweeps;
+        // the FP64 factors only in the FP64 form
+        dalloc(&c->A, nn);
         dalloc(&c->LU, mixed ? 1 : nn);
-        dalloc(&c->F, mixed ? 1 : nn);
+        dalloc(&c->F, nn);
         if (mixed) {
             dalloc(&c->A32, nn);
             dalloc(&c->LU32, nn);
             dalloc(&c->lu32_p0, (size_t)n * 32);
             dalloc(&c->lu32_q, (size_t)n * 64);
-            double **mv[] = {&c->m_vacc, &c->m_subacc, &c->m_g, &c->m_r, &c->m_dx, &c->m_dx2};
+            double **mv[] = {&c->m_g, &c->m_r, &c->m_dx, &c->m_dx2};
             for (double **v : mv) dalloc(v, (size_t)n);
             dalloc(&c->m_cnt, (size_t)(n + 255) / 256);
             D4_CUDA_OK(cudaMemset(c->m_cnt, 0, sizeof(unsigned) * ((n + 255) / 256)));
+            dalloc(&c->m_conv, (size_t)d4::kIrMax + 1);
             dalloc(&c->m_c32, (size_t)n);
             dalloc(&c->m_w1, (size_t)n);
             dalloc(&c->m_part, (size_t)((n + 255) / 256) * n);
-            dalloc(&c->m_pp, (size_t)4 * ((n + 31) / 32) * n);
             dalloc(&c->m_resid, 16);
             D4_CUDA_OK(cudaMemset(c->m_resid, 0, sizeof(unsigned long long) * 16));
-            D4_CUDA_OK(cudaMemset(c->A32, 0, sizeof(float) * nn));
+            std::vector<int> ident(n);
+            for (int i = 0; i < n; ++i) ident[i] = i;
+            dalloc(&c->spiv, (size_t)n);
+            D4_CUDA_OK(cudaMemcpy(c->spiv, ident.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
             c->lu32_grid = d4::coop_grid_size32(n);
             if (c->lu32_grid < 0) throw d4::StateError("n too large for the cooperative LU");
             const std::vector<int> sched = d4::blu_schedule(n);
@@ -797,10 +782,8 @@ int d4_create(void **out, int n, const d4_params *p) {
         D4_CUDA_OK(cudaMemset(c->wave_err, 0, sizeof(int) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_red, sizeof(double) * 8));
         D4_CUDA_OK(cudaMallocHost((void **)&c->h_flags, sizeof(int) * d4::kFlagCount));
-        if (!mixed) {
-            D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
-            D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
-        }
+        D4_CUDA_OK(cudaMemset(c->A, 0, sizeof(double) * nn));
+        D4_CUDA_OK(cudaMemset(c->F, 0, sizeof(double) * nn));
         D4_CUDA_OK(cudaMemset(c->dvec, 0, sizeof(double) * n));
         D4_CUDA_OK(cudaMemset(c->flags, 0, sizeof(int) * d4::kFlagCount));
         c->lu_grid = d4::coop_grid_size(n);
@@ -838,6 +821,9 @@ int d4_create(void **out, int n, const d4_params *p) {
                 dalloc(&c->F_b, nn);
             } else {
                 d4::Mix32Bufs &B = c->m32b;
+                dalloc(&c->F_b, nn);
+                dalloc(&B.A64, nn);
+                dalloc(&B.conv, (size_t)d4::kIrMax + 1);
                 dalloc(&B.A32, nn);
                 dalloc(&B.LU32, nn);
                 dalloc(&B.P0, (size_t)n * 32);
@@ -860,8 +846,6 @@ int d4_create(void **out, int n, const d4_params *p) {
                 B.resid_count = &c->m_resid_count_b;
                 B.blk = &c->m_blk_b;
                 d4::blu_alloc(B.blu, n, c->blu_tasks, &c->blu_state_b);
-                dalloc(&c->m_vacc_b, (size_t)n);
-                dalloc(&c->m_pp_b, (size_t)4 * ((n + 31) / 32) * n);
             }
         }
         d4::reset_tol64(*c);
@@ -945,10 +929,7 @@ int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, doub
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, x);
     upload(*c, c->ys_tmp, y);
-    if (c->p.precision == D4_PREC_MIXED)
-        d4::speeds32(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
-    else
-        d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
+    d4::speeds64(*c, c->xs_tmp, c->ys_tmp, ext_stress(c->p.protocol, sim_time), c->speed2);
     download(*c, v, c->speed2);
     if (tol) download(*c, tol, c->tol);
     read_async_errors(*c);
@@ -964,12 +945,8 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
     D4_GUARD_BEGIN
     upload(*c, c->xs_tmp, x);
     upload(*c, c->ys_tmp, y);
-    if (c->p.precision == D4_PREC_MIXED)
-        d4::jacobian32(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
-                       ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
-    else
-        d4::jacobian64(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
-                       ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
+    d4::jacobian64(*c, c->xs_tmp, c->ys_tmp, stepsize, ext_stress(c->p.protocol, t_a),
+                   ext_stress(c->p.protocol, t_b), c->v_init, c->speed);
     download(*c, v_a, c->v_init);
     download(*c, v_b, c->speed);
     if (dvec) download(*c, dvec, c->dvec);
@@ -984,10 +961,7 @@ int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *
     Ctx *c = (Ctx *)ctx;
     if (!c) return D4_ERR_ARG;
     D4_GUARD_BEGIN
-    if (c->p.precision == D4_PREC_MIXED)
-        d4::jacobian_from_prev32(*c, factor);
-    else
-        d4::jacobian_from_prev64(*c, factor);
+    d4::jacobian_from_prev64(*c, factor);
     if (dvec) download(*c, dvec, c->dvec);
     copy_matrix_out(*c, a_colmajor);
     sync(*c);
@@ -1000,15 +974,6 @@ int d4_set_matrix(void *ctx, const double *a_colmajor) {
     if (!c || !a_colmajor) return D4_ERR_ARG;
     D4_GUARD_BEGIN
     const size_t nn = (size_t)c->n * c->n;
-    if (c->p.precision == D4_PREC_MIXED) {
-        // the mixed form's matrix is FP32 (rounded to nearest)
-        std::vector<float> a32(nn);
-        for (size_t k = 0; k < nn; ++k) a32[k] = (float)a_colmajor[k];
-        D4_CUDA_OK(cudaMemcpyAsync(c->A32, a32.data(), sizeof(float) * nn,
-                                   cudaMemcpyHostToDevice, c->stream));
-        sync(*c);
-        return D4_OK;
-    }
     D4_CUDA_OK(cudaMemcpyAsync(c->A, a_colmajor, sizeof(double) * nn, cudaMemcpyHostToDevice,
                                c->stream));
     sync(*c);
@@ -1076,10 +1041,7 @@ int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, doub
     const size_t b = sizeof(double) * (size_t)count;
     cudaMemcpyAsync(d, dx, b, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(d + count, dy, b, cudaMemcpyHostToDevice, c->stream);
-    if (c->p.precision == D4_PREC_MIXED)
-        d4::field_eval_mixed(*c, count, d, d + count, d + 2 * count, d + 3 * count);
-    else
-        d4::field_eval64(*c, count, d, d + count, d + 2 * count, d + 3 * count);
+    d4::field_eval64(*c, count, d, d + count, d + 2 * count, d + 3 * count);
     cudaMemcpyAsync(xy, d + 2 * count, b, cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(xyd, d + 3 * count, b, cudaMemcpyDeviceToHost, c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);

@@ -475,6 +475,9 @@ struct SolveArgs {
     int *ticket;       // ticket counter (0 at the launch; the CTA taking the last ticket resets it)
     int epoch;
     int *flags;        // kFlagBarrierTimeout
+    const int *perm;   // rows of P (the block LU factorised P A); null: identity
+    const unsigned long long *conv;  // refinement: max|g|, then max|r| after each sweep
+    int it;            // refinement sweep of this solve
 };
 
 __device__ __forceinline__ void load_slice(const SolveArgs &s, int ti, int tj, int r2, int cg,
@@ -531,7 +534,7 @@ __device__ __forceinline__ void solve_block(const SolveArgs &s, int i, float (*r
         const int gr = i * kB + tid;
         float base;
         if (kFwd)
-            base = gr < s.n ? (float)s.b[gr] : 0.f;
+            base = gr < s.n ? (float)s.b[s.perm ? s.perm[gr] : gr] : 0.f;
         else
             base = __ldcg(s.y + gr);
         const float z = base - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
@@ -577,6 +580,12 @@ __global__ void __launch_bounds__(kThreads) k_bsolve32(SolveArgs s) {
     }
     __syncthreads();
     const int t = tk_s;
+    if (s.it > 0) {
+        // the previous refinement sweep already met its tolerance: nothing to do
+        const double g = __longlong_as_double((long long)__ldcg(s.conv));
+        const double r = __longlong_as_double((long long)__ldcg(s.conv + s.it));
+        if (r <= kIrStop * g) return;
+    }
     if (t < T)
         solve_block<true>(s, t, red, zs);
     else if (t < 2 * T)
@@ -679,8 +688,8 @@ void blu_factor_async(const BluBufs &B, int n, const float *A, float *LU, int *f
     check_launch("k_blu32");
 }
 
-void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, int *flags,
-                     cudaStream_t st) {
+void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, const int *perm,
+                     const unsigned long long *conv, int it, int *flags, cudaStream_t st) {
     const int T = blu_tiles(n);
     blu::SolveArgs s;
     s.n = n;
@@ -694,6 +703,9 @@ void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, 
     s.ticket = B.ticket + 1;
     s.epoch = ++B.state->solve_epoch;
     s.flags = flags;
+    s.perm = perm;
+    s.conv = conv;
+    s.it = it;
     blu::k_bsolve32<<<2 * T, blu::kThreads, 0, st>>>(s);
     check_launch("k_bsolve32");
 }

@@ -62,12 +62,14 @@ struct BluBufs {
 // matrix the refinement's residual multiplies, the factors and the pivot
 // bookkeeping, the refinement vectors and the ring of residual maxima.
 struct Mix32Bufs {
+    double *A64 = nullptr;  // the FP64 matrix the refinement's residual multiplies
     float *A32 = nullptr, *LU32 = nullptr, *P0 = nullptr, *Q = nullptr;
     unsigned *mask = nullptr, *bar = nullptr;
     int *flags = nullptr, *perm = nullptr, *piv = nullptr;
     double *g = nullptr, *r = nullptr, *dx = nullptr, *dx2 = nullptr;
     double *part = nullptr;  // ceil(n / 256) x n: the residual product's column-chunk sums
     unsigned *cnt = nullptr; // ceil(n / 256): chunk blocks finished per row block (k_resid_fused)
+    unsigned long long *conv = nullptr;  // kIrMax + 1: max|g|, then max|r| after each sweep
     float *c32 = nullptr, *w1 = nullptr;
     unsigned long long *resid = nullptr;  // 8 pairs (max |r|, max |g|)
     int *resid_count = nullptr;           // host: next slot of resid
@@ -151,12 +153,12 @@ struct Ctx {
     // mixed form: FP32 matrix and factors, FP64 accumulators and refinement
     float *A32 = nullptr, *LU32 = nullptr, *lu32_p0 = nullptr, *lu32_q = nullptr;
     int lu32_grid = 0;
-    double *m_vacc = nullptr, *m_subacc = nullptr, *m_g = nullptr, *m_r = nullptr,
-           *m_dx = nullptr, *m_dx2 = nullptr;
+    double *m_g = nullptr, *m_r = nullptr, *m_dx = nullptr, *m_dx2 = nullptr;
     unsigned *m_cnt = nullptr;
+    unsigned long long *m_conv = nullptr;
+    int *spiv = nullptr;  // static pivots of the block LU: row of A at each position of P A
     float *m_c32 = nullptr, *m_w1 = nullptr;
     double *m_part = nullptr;  // residual product's column-chunk sums (Mix32Bufs::part)
-    double *m_pp = nullptr, *m_pp_b = nullptr;  // pair-tile row partials, 4 x ceil(n/32) x n
     unsigned long long *m_resid = nullptr;  // 8 pairs (max |r|, max |g|) of recent solves
     int m_resid_count = 0;
     int ir_iters = 2;
@@ -202,9 +204,8 @@ struct Ctx {
     double *F_b = nullptr, *dvec_b = nullptr, *speed_b = nullptr, *speed2_b = nullptr,
            *xw1_b = nullptr, *xw2_b = nullptr, *dx_b = nullptr;
     int *flags3 = nullptr;  // 3 x kFlagCount
-    // mixed form: stage I's FP32 buffers and pair-sum scratch
+    // mixed form: stage I's FP64 matrix copy and FP32 buffers
     Mix32Bufs m32b;
-    double *m_vacc_b = nullptr;
     int m_resid_count_b = 0;
 
     // pair-tile autotuner (FP64 pair kernels): threads per 32x32 tile along j
@@ -296,30 +297,26 @@ void solve_plain64(Ctx &c, const double *g);
 void solve_plain32(Ctx &c, const double *g);
 
 // ---- mixed form (d4_mixed.cu) ----
-void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v);
-void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
-                double *v_a, double *v_b);
-void jacobian_from_prev32(Ctx &c, double factor);
-// The context's own FP32 buffers (stages II and III, and the sequential attempt).
+// Refinement sweeps: at most kIrMax, stopping once max|r| <= kIrStop max|g|.
+constexpr int kIrMax = 4;
+constexpr double kIrStop = 1e-12;
+// The context's own buffers (stages II and III, and the sequential attempt).
 Mix32Bufs primary_mix32(Ctx &c);
-// FP32 factorisation into B.LU32 on `st` with `grid` CTAs, without waiting;
-// with copy_matrix, A is also copied into B.A32 (the refinement's matrix).
-// `after_copy` (may be null) is recorded once A has been copied.
-void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix, int grid,
+// FP32 factorisation of the FP64 matrix A into B on `st` with up to `grid`
+// CTAs, without waiting; with copy_matrix, A is first copied into B.A64 (the
+// matrix stage I's refinement multiplies) and `after_copy` (may be null) is
+// recorded once it is taken.
+void factor32_async(Ctx &c, const Mix32Bufs &B, const double *A, bool copy_matrix, int grid,
                     cudaStream_t st, cudaEvent_t after_copy);
+// The primary buffers' last pivoted factorisation gives the block LU's pivots.
+void adopt_pivots(Ctx &c);
 // solve_update32 with explicit buffers, weights, correction output and stream.
 void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
                          cudaStream_t st, int gmode, double hval, const double *s_end,
                          const double *s_init, const double *x_new, const double *x_old,
                          const double *base, double *out);
-// speeds32 with its own pair-sum scratch (row sums, tile partials) on `st`.
-void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const double *x,
-                   const double *y, double ext, double *v);
 int factor32(Ctx &c);
 int coop_grid_size32(int n);
-// The mixed form's field at points: FP64 stress, FP32 gradient.
-void field_eval_mixed(Ctx &c, int count, const double *dx, const double *dy, double *xy,
-                      double *xyd);
 
 // ---- mixed form's block LU (d4_blu32.cu) ----
 constexpr double kRefineLimit = 1e-9;  // refined max|r| / max|g| above this: exact path
@@ -336,9 +333,11 @@ void blu_factor_async(const BluBufs &B, int n, const float *A, float *LU, int *f
                       cudaStream_t st);
 // Runs a bounded wait on a barrier or flag that nothing completes (d4_wait_selftest).
 int wait_selftest(int which);
-// x = (block LU)^-1 b in FP32 (b FP64); the result is B.xs (padded to 128-row blocks).
-void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, int *flags,
-                     cudaStream_t st);
+// x = (block LU of P A)^-1 P b in FP32 (b FP64; perm: the rows of P, null for
+// the identity); the result is B.xs (padded to 128-row blocks).  Refinement
+// sweep `it`: returns at once when conv says sweep it - 1 converged.
+void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, const int *perm,
+                     const unsigned long long *conv, int it, int *flags, cudaStream_t st);
 void solve_update32(Ctx &c, int gmode, double hval, const double *s_end, const double *s_init,
                     const double *x_new, const double *x_old, const double *base, double *out);
 

@@ -1,21 +1,30 @@
 // d4_mixed.cu: the mixed-precision form of the implicit step.
 //
-// Pair stress gradient in FP32 (d4_field32.cuh: compensated image sums,
-// cancellation-free central image), each unique pair once per sweep, summed
-// into FP64 accumulators.  The pair stress itself, whose sums are the speeds
-// that enter the Newton residual g, is the FP64 field: speeds from the FP32
-// field (about 1e-6 relative) moved positions by 1.9e-8 from the FP64 form
-// within 8 steps at N=4096, while the gradient only shapes the matrix, whose
-// error the refined solves remove.  The dense Jacobian A = I + D J is kept in FP32 and
-// factorised in FP32 (the cooperative LU of d4_lu_coop.cuh).  FP64 is kept for
-// positions, speeds, residuals g, d_i, the position updates and the error ratio;
-// each solve is refined in FP64 against the stored FP32 matrix:
-//     dx = 0, r = g;  repeat: c = LU32 \ r;  dx += c;  r = g - A32 dx
-// so the solution of A32 dx = g is accurate to FP64 rounding times cond(A).
+// The speeds, the Jacobian A = I + D J, the residuals g, the position updates
+// and the error ratio are the FP64 form's (its exact-order sweeps, d4_fp64.cu):
+// the quantities that decide where the dislocations go stay FP64.  What runs
+// in lower precision is the linear algebra that dominates the step: A is
+// rounded to FP32 and factorised by the block LU on the tensor cores
+// (d4_blu32.cu, 3xTF32 products; or the pivoted cooperative LU), and each
+// solve is refined in FP64 against the FP64 matrix:
+//     dx = 0, r = g;  repeat: c = LU32^-1 r (FP32);  dx += c;  r = g - A dx (FP64)
+// until max|r| <= kIrStop max|g| (checked on the device: later sweeps return
+// at once) or kIrMax sweeps.  The refined dx is the solution of A dx = g to
+// that residual, so positions follow the FP64 form's Newton iterations.  A
+// Jacobian taken from the FP32 field instead (about 1e-6 relative) moved
+// positions 1.7e-8 from the FP64 form within 10 steps at N=4096 and 1e-6
+// within 20: the two-iteration scheme of src/simulation.cpp:100-150 passes the
+// matrix's error on to the positions, so the matrix the residual multiplies
+// must be the FP64 one.
+//
+// Static pivoting: the block LU factorises P A, with P the row permutation of
+// the context's last pivoted (exact partial pivoting) factorisation, identity
+// until one ran; an attempt whose block factorisation fails (a bad pivot in a
+// diagonal tile, or a residual left above kRefineLimit) is redone with the
+// pivoted LU, whose permutation the next block LUs then use.
 #include <cstdint>
 #include <utility>
 
-#include "d4_field32.cuh"
 #include "d4_field64.cuh"
 #include "d4_lu_coop.cuh"
 #include "d4_trsv.cuh"
@@ -23,215 +32,84 @@
 namespace d4 {
 namespace {
 
-__device__ __forceinline__ double bsign(int i, int n) { return i < n / 2 ? 1.0 : -1.0; }
-
-__device__ __forceinline__ void tol_min(double *tol, int idx, double d) {
-    atomicMin(reinterpret_cast<unsigned long long *>(tol + idx),
-              static_cast<unsigned long long>(__double_as_longlong(d)));
-}
-
-__device__ __forceinline__ void tile_of(int t, int T, int &ti, int &tj) {
-    int r = 0, rem = t;
-    while (rem >= T - r) {
-        rem -= T - r;
-        ++r;
-    }
-    ti = r;
-    tj = r + rem;
-}
-
-struct Pair32Args {
-    int n;
-    const double *x, *y;
-    double *vacc;    // FP64 sum of signed forces per dislocation (k_rowsum32)
-    double *subacc;  // FP64 sum of -J_ij per row (k_rowsum32; fused sweep)
-    double *part;    // 4 x T x n tile partials: [0] forces as row i, [1] as row j,
-                     // [2] -J as row i, [3] -J as row j (slot = the other tile index)
-    float *A;        // raw J entries (fused sweep)
-    double *tol;
-    double min_prec_sq, h, cut_sq, cutoff, range_sq, one_per_cut_sq;
-    int heaviside;
-};
-
-// Unique pairs in 32x32 tiles (upper triangle); lanes walk i, threadIdx.y
-// steps j.  Row sums over the tile's j go through shared memory, column sums
-// over i through warp shuffles; each tile stores one partial per row it
-// touches (no atomics), and k_rowsum32 adds them in tile order, so the sums
-// are the same on every run.
-template <bool kJac>
-__global__ void __launch_bounds__(256) k_pairs32(Pair32Args a) {
-    const int T = (a.n + 31) / 32;
-    int ti, tj;
-    tile_of(blockIdx.x, T, ti, tj);
-    __shared__ double sxi[32], syi[32], sxj[32], syj[32];
-    __shared__ double rs[8][33], rj[8][33];
-    __shared__ float sv[kJac ? 32 : 1][kJac ? 33 : 1];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i0 = ti * 32, j0 = tj * 32;
-    if (ty == 0) {
-        const int i = i0 + tx, j = j0 + tx;
-        sxi[tx] = i < a.n ? a.x[i] : 0;
-        syi[tx] = i < a.n ? a.y[i] : 0;
-        sxj[tx] = j < a.n ? a.x[j] : 0;
-        syj[tx] = j < a.n ? a.y[j] : 0;
-    }
-    __syncthreads();
-    const int i = i0 + tx;
-    const double bi = bsign(i, a.n);
-    double row_f = 0, row_j = 0, row_min = 1e300;
-    for (int lj = ty; lj < 32; lj += 8) {
-        const int j = j0 + lj;
-        double f = 0, fj = 0;
-        float v = 0.f;
-        const bool ok = i < a.n && j < a.n && i < j;
-        if (ok) {
-            const double dx = f64::normalize(sxi[tx] - sxj[lj]);
-            const double dy = f64::normalize(syi[tx] - syj[lj]);
-            const double dist_sq = dx * dx + dy * dy;
-            if (a.tol && dist_sq < a.min_prec_sq) {
-                row_min = fmin(row_min, dist_sq);
-                tol_min(a.tol, j, dist_sq);
-            }
-            // the force enters the Newton residual: FP64 field (an FP32 force,
-            // ~1e-6 relative, moved positions by ~1e-8 within a few steps)
-            const double bj = bsign(j, a.n);
-            f = f64::xy(dx, dy, f64::Hyp(f64::exp2pix(dx)), f64::cos2piy(dy)) * bi * bj;
-            if (kJac && dist_sq < a.range_sq * a.cut_sq) {
-                // the gradient only builds the matrix: FP32, compensated
-                float s, sd;
-                f32::field<true>((float)dx, (float)dy, s, sd);
-                double vv = a.h * bj * bi * (double)sd;
-                if (!a.heaviside && dist_sq > a.cut_sq) {
-                    const double t = sqrt(dist_sq) - a.cutoff;
-                    vv *= exp(-(t * t) * a.one_per_cut_sq);
-                }
-                v = (float)vv;
-                fj = vv;
-            }
-            if (kJac) a.A[(size_t)i + (size_t)j * a.n] = v;
-        }
-        if (kJac) sv[tx][lj] = v;
-        row_f += f;
-        row_j += fj;
-        // column sums for row j: -f and -J, reduced over the warp's lanes (i)
-        double cf = -f, cj = fj;
-        for (int o = 16; o > 0; o >>= 1) {
-            cf += __shfl_down_sync(0xffffffffu, cf, o);
-            if (kJac) cj += __shfl_down_sync(0xffffffffu, cj, o);
-        }
-        if (tx == 0 && j < a.n) {
-            a.part[((size_t)T + ti) * a.n + j] = cf;
-            if (kJac) a.part[((size_t)3 * T + ti) * a.n + j] = -cj;
-        }
-    }
-    if (a.tol && i < a.n && row_min < a.min_prec_sq) tol_min(a.tol, i, row_min);
-    rs[ty][tx] = row_f;
-    rj[ty][tx] = row_j;
-    __syncthreads();
-    if (ty == 0 && i < a.n) {
-        double sf = 0, sj = 0;
-        for (int k = 0; k < 8; ++k) {
-            sf += rs[k][tx];
-            sj += rj[k][tx];
-        }
-        a.part[(size_t)tj * a.n + i] = sf;
-        if (kJac) a.part[((size_t)2 * T + tj) * a.n + i] = -sj;
-    }
-    if (kJac) {
-        const int j = j0 + tx;
-        for (int li = ty; li < 32; li += 8) {
-            const int ii = i0 + li;
-            if (ii < a.n && j < a.n && ii < j) a.A[(size_t)j + (size_t)ii * a.n] = sv[li][tx];
-        }
-    }
-}
-
-// Row r's partials in tile order: as row j of the tiles (tr, r/32), tr <= r/32,
-// then as row i of the tiles (r/32, tj), tj >= r/32.
-template <bool kJac>
-__global__ void k_rowsum32(int n, const double *part, double *vacc, double *subacc) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    const int T = (n + 31) / 32, R = r / 32;
-    double v = 0, w = 0;
-    for (int t = 0; t <= R; ++t) {
-        v += part[((size_t)T + t) * n + r];
-        if (kJac) w += part[((size_t)3 * T + t) * n + r];
-    }
-    for (int t = R; t < T; ++t) {
-        v += part[(size_t)t * n + r];
-        if (kJac) w += part[((size_t)2 * T + t) * n + r];
-    }
-    vacc[r] = v;
-    if (kJac) subacc[r] = w;
-}
-
-__global__ void k_speed_fin32(int n, const double *vacc, double ext, double *v) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = vacc[i] + ext * bsign(i, n);
-}
-
-// Row i: speeds at both times, d_i = weight(subSum_i), row scale and diagonal.
-__global__ void k_jac_fin32(int n, const double *vacc, const double *subacc, double ext_a,
-                            double ext_b, double *v_a, double *v_b, double *dvec, double *sc,
-                            float *A, char wfn) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double b = bsign(i, n);
-    v_a[i] = vacc[i] + ext_a * b;
-    v_b[i] = vacc[i] + ext_b * b;
-    const double sub = subacc[i];
-    const double d = f64::weight(sub, wfn);
-    dvec[i] = d;
-    const double s = (1 + d) / 2;
-    sc[i] = s;
-    A[(size_t)i + (size_t)i * n] = (float)(sub * s + 1);
-}
-
-// A_rc *= sc_r off the diagonal (column-major, 2-D grid).
-__global__ void k_scale_rows32(int n, float *A, const double *sc) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = blockIdx.y;
-    if (r < n && r != c) A[(size_t)r + (size_t)c * n] = (float)((double)A[(size_t)r + (size_t)c * n] * sc[r]);
-}
-
-// Half-step rescale on the FP32 matrix (src/simulation.cpp:584-594).
-__global__ void k_half_rescale32(int n, float *A, const double *fac) {
+// FP64 matrix -> FP32, rows gathered through perm (null: identity):
+// A32[r + c n] = A[perm[r] + c n].
+__global__ void k_to32(int n, const double *__restrict__ A, const int *__restrict__ perm,
+                       float *__restrict__ A32) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (r >= n) return;
-    const double f = fac[r];
-    const double e = A[(size_t)r + (size_t)c * n];
-    A[(size_t)r + (size_t)c * n] = (float)((r == c) ? 1 + (e - 1) / 2 * f : e / 2 * f);
+    const int src = perm ? perm[r] : r;
+    A32[(size_t)r + (size_t)c * n] = (float)A[(size_t)src + (size_t)c * n];
 }
 
-// g of the stage (as the FP64 form), r = g, dx = 0.
-__global__ void k_ir_init(int n, trsv::GArgs ga, double *g, double *r, double *dx) {
+__device__ __forceinline__ unsigned long long obits(double v) {
+    return (unsigned long long)__double_as_longlong(v);  // ordered for v >= 0
+}
+
+// max over the block of v (>= 0) into *out by atomicMax on the bit pattern.
+__device__ void block_absmax(double v, unsigned long long *out) {
+    __shared__ double wm[8];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wm[w]);
+        atomicMax(out, obits(m));
+    }
+}
+
+// g of the stage (as the FP64 form), r = g, dx = 0, max|g| into conv[0]
+// (conv zeroed before the launch).
+__global__ void __launch_bounds__(256) k_ir_init(int n, trsv::GArgs ga, double *g, double *r,
+                                                 double *dx, unsigned long long *conv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double gi = trsv::g_of(ga, i);
-    g[i] = gi;
-    r[i] = gi;
-    dx[i] = 0;
+    double a = 0;
+    if (i < n) {
+        const double gi = trsv::g_of(ga, i);
+        g[i] = gi;
+        r[i] = gi;
+        dx[i] = 0;
+        a = fabs(gi);
+    }
+    block_absmax(a, conv);
 }
 
-// One refinement update in one launch: dx_out = dx + c and r = g - A32 dx_out.
-// Block (x, y) multiplies rows 256x.. by column chunk y (FP64 accumulation in
-// column order, the chunk's corrected dx staged in shared memory; the blocks of
-// row block 0 also store it to dx_out, a buffer no block reads) into
-// part[y][i]; the last block of each row block to finish (a counter per row
-// block, reset by that block) subtracts the chunk sums from g in chunk order.
-// The arithmetic and its order are those of a separate update, product and
-// residual, so the residual is the same on every run.
-__global__ void __launch_bounds__(256) k_resid_fused(int n, const float *__restrict__ A,
+__device__ __forceinline__ bool converged(const unsigned long long *conv, int done) {
+    // after `done` sweeps (done >= 1): max|r| of the last one against max|g|
+    if (done < 1) return false;
+    const double g = __longlong_as_double((long long)__ldcg(conv));
+    const double r = __longlong_as_double((long long)__ldcg(conv + done));
+    return r <= kIrStop * g;
+}
+
+// One refinement sweep's update in one launch: dx_out = dx + c and
+// r = g - A dx_out with the FP64 matrix.  Block (x, y) multiplies rows 256x..
+// by column chunk y (FP64, column order, the chunk's corrected dx staged in
+// shared memory; the blocks of row block 0 also store it to dx_out, a buffer
+// no block reads) into part[y][i]; the last block of each row block to finish
+// (a counter per row block, reset by that block) subtracts the chunk sums from
+// g in chunk order and adds its rows' max|r| to conv[it + 1].  The order of
+// every sum is fixed, so the residual is the same on every run.  When the
+// previous sweep already converged the launch only carries dx over.
+__global__ void __launch_bounds__(256) k_resid_fused(int n, const double *__restrict__ A,
                                                      const double *__restrict__ dx,
                                                      const float *__restrict__ corr,
                                                      double *dx_out, const double *g,
                                                      double *part, int chunk, int nch,
-                                                     unsigned *cnt, double *r) {
+                                                     unsigned *cnt, double *r,
+                                                     unsigned long long *conv, int it) {
     __shared__ double sdx[256];
     __shared__ int last;
     const int c0 = blockIdx.y * chunk, c1 = min(n, c0 + chunk);
+    if (converged(conv, it)) {
+        if (blockIdx.x == 0)
+            for (int t = threadIdx.x; t < c1 - c0; t += blockDim.x) dx_out[c0 + t] = dx[c0 + t];
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+            atomicMax(conv + it + 1, __ldcg(conv + it));
+        return;
+    }
     for (int t = threadIdx.x; t < c1 - c0; t += blockDim.x) {
         const double v = dx[c0 + t] + (double)corr[c0 + t];
         sdx[t] = v;
@@ -241,7 +119,7 @@ __global__ void __launch_bounds__(256) k_resid_fused(int n, const float *__restr
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         double s = 0;
-        for (int c = c0; c < c1; ++c) s += (double)__ldg(A + (size_t)i + (size_t)c * n) * sdx[c - c0];
+        for (int c = c0; c < c1; ++c) s += __ldg(A + (size_t)i + (size_t)c * n) * sdx[c - c0];
         part[(size_t)blockIdx.y * n + i] = s;
     }
     __threadfence();
@@ -250,12 +128,15 @@ __global__ void __launch_bounds__(256) k_resid_fused(int n, const float *__restr
     __syncthreads();
     if (!last) return;
     __threadfence();
+    double a = 0;
     if (i < n) {
         double v = g[i];
         for (int q = 0; q < nch; ++q) v = v - __ldcg(part + (size_t)q * n + i);
         r[i] = v;
+        a = fabs(v);
     }
     if (threadIdx.x == 0) cnt[blockIdx.x] = 0;
+    block_absmax(a, conv + it + 1);
 }
 
 // max |r| and max |g| into out[0], out[1] (as ordered bits of non-negatives).
@@ -270,8 +151,8 @@ __global__ void k_absmax2(int n, const double *r, const double *g, unsigned long
         m2 = fmax(m2, __shfl_down_sync(0xffffffffu, m2, o));
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicMax(out, (unsigned long long)__double_as_longlong(m1));
-        atomicMax(out + 1, (unsigned long long)__double_as_longlong(m2));
+        atomicMax(out, obits(m1));
+        atomicMax(out + 1, obits(m2));
     }
 }
 
@@ -286,97 +167,13 @@ __global__ void k_ir_apply(int n, const double *dx, const int *flags, const doub
     out[i] = base[i] - d;
 }
 
-// The mixed form's field at single points: the FP64 stress its speeds use and
-// the FP32 gradient its matrix uses (the same calls as k_pairs32).
-__global__ void k_field_mixed(int count, const double *dx, const double *dy, double *xy,
-                              double *xyd) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    const double x = dx[k], y = dy[k];
-    xy[k] = f64::xy(x, y, f64::Hyp(f64::exp2pix(x)), f64::cos2piy(y));
-    float s, sd;
-    f32::field<true>((float)x, (float)y, s, sd);
-    xyd[k] = (double)sd;
-}
-
 inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-void field_eval_mixed(Ctx &c, int count, const double *dx, const double *dy, double *xy,
-                      double *xyd) {
-    k_field_mixed<<<nb(count, 128), 128, 0, c.stream>>>(count, dx, dy, xy, xyd);
-    check_launch("k_field_mixed");
-}
-
-static Pair32Args pair32(Ctx &c, const double *x, const double *y) {
-    Pair32Args a;
-    a.n = c.n;
-    a.x = x;
-    a.y = y;
-    a.vacc = c.m_vacc;
-    a.subacc = c.m_subacc;
-    a.part = c.m_pp;
-    a.A = c.A32;
-    a.tol = c.use_dipole ? c.tol : nullptr;
-    a.min_prec_sq = c.min_prec_sq;
-    a.h = 0;
-    a.cut_sq = c.cutoff_sq;
-    a.cutoff = c.cutoff;
-    a.range_sq = c.range_sq;
-    a.one_per_cut_sq = 1 / c.cutoff_sq;
-    a.heaviside = c.p.heaviside_cutoff;
-    return a;
-}
-
-static int pair_tiles(int n) {
-    const int T = (n + 31) / 32;
-    return T * (T + 1) / 2;
-}
-
-void speeds32_with(Ctx &c, double *vacc, double *part, cudaStream_t st, const double *x,
-                   const double *y, double ext, double *v) {
-    Pair32Args a = pair32(c, x, y);
-    a.vacc = vacc;
-    a.part = part;
-    k_pairs32<false><<<pair_tiles(c.n), dim3(32, 8), 0, st>>>(a);
-    check_launch("k_pairs32<speeds>");
-    k_rowsum32<false><<<nb(c.n, 256), 256, 0, st>>>(c.n, part, vacc, nullptr);
-    check_launch("k_rowsum32<speeds>");
-    k_speed_fin32<<<nb(c.n, 256), 256, 0, st>>>(c.n, vacc, ext, v);
-    check_launch("k_speed_fin32");
-}
-
-void speeds32(Ctx &c, const double *x, const double *y, double ext, double *v) {
-    speeds32_with(c, c.m_vacc, c.m_pp, c.stream, x, y, ext, v);
-}
-
-void jacobian32(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
-                double *v_a, double *v_b) {
-    Pair32Args a = pair32(c, x, y);
-    a.h = h;
-    k_pairs32<true><<<pair_tiles(c.n), dim3(32, 8), 0, c.stream>>>(a);
-    check_launch("k_pairs32<jacobian>");
-    k_rowsum32<true><<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_pp, c.m_vacc, c.m_subacc);
-    check_launch("k_rowsum32<jacobian>");
-    k_jac_fin32<<<nb(c.n, 256), 256, 0, c.stream>>>(c.n, c.m_vacc, c.m_subacc, ext_a, ext_b,
-                                                     v_a, v_b, c.dvec, c.fac, c.A32,
-                                                     c.p.weight_function);
-    check_launch("k_jac_fin32");
-    k_scale_rows32<<<dim3(nb(c.n, 256), c.n), 256, 0, c.stream>>>(c.n, c.A32, c.fac);
-    check_launch("k_scale_rows32");
-}
-
-void jacobian_from_prev32(Ctx &c, double factor) {
-    half_weights64(c, factor);  // dvec_new, fac
-    k_half_rescale32<<<dim3(nb(c.n, 256), c.n), 256, 0, c.stream>>>(c.n, c.A32, c.fac);
-    check_launch("k_half_rescale32");
-    D4_CUDA_OK(cudaMemcpyAsync(c.dvec, c.dvec_new, sizeof(double) * c.n, cudaMemcpyDeviceToDevice,
-                               c.stream));
-}
-
 Mix32Bufs primary_mix32(Ctx &c) {
     Mix32Bufs B;
+    B.A64 = c.A;
     B.A32 = c.A32;
     B.LU32 = c.LU32;
     B.P0 = c.lu32_p0;
@@ -391,6 +188,7 @@ Mix32Bufs primary_mix32(Ctx &c) {
     B.dx = c.m_dx;
     B.dx2 = c.m_dx2;
     B.cnt = c.m_cnt;
+    B.conv = c.m_conv;
     B.part = c.m_part;
     B.c32 = c.m_c32;
     B.w1 = c.m_w1;
@@ -401,26 +199,36 @@ Mix32Bufs primary_mix32(Ctx &c) {
     return B;
 }
 
-void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix, int grid,
+// Factorisation of the FP64 matrix A (column-major n x n) into B: with
+// copy_matrix, A is first copied into B.A64 (stage I's own FP64 matrix, which
+// its refinement multiplies while stage II rescales A) and `after_copy` (may
+// be null) is recorded once that copy is taken.  The block LU factorises the
+// FP32 rounding of P A (P: the static pivots c.spiv); the pivoted cooperative
+// LU that of A.  Queued on `st` without waiting.
+void factor32_async(Ctx &c, const Mix32Bufs &B, const double *A, bool copy_matrix, int grid,
                     cudaStream_t st, cudaEvent_t after_copy) {
     const int n = c.n;
-    const size_t bytes = sizeof(float) * (size_t)n * n;
+    const size_t nn = (size_t)n * n;
+    const double *src = A;
+    if (copy_matrix) {
+        D4_CUDA_OK(cudaMemcpyAsync(B.A64, A, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+        src = B.A64;
+    }
+    if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
+    D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
     *B.blk = c.m_fast;
     if (c.m_fast) {
-        // block LU (d4_blu32.cu): reads the matrix, writes the factors and operands
-        D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
-        if (copy_matrix) D4_CUDA_OK(cudaMemcpyAsync(B.A32, A, bytes, cudaMemcpyDeviceToDevice, st));
-        if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
-        blu_factor_async(B.blu, n, copy_matrix ? B.A32 : A, B.LU32, B.flags, grid, st);
+        // block LU (d4_blu32.cu) of the row-permuted FP32 matrix
+        k_to32<<<dim3(nb(n, 256), n), 256, 0, st>>>(n, src, c.spiv, B.A32);
+        check_launch("k_to32");
+        blu_factor_async(B.blu, n, B.A32, B.LU32, B.flags, grid, st);
         ++c.m_blocklu;
         return;
     }
-    D4_CUDA_OK(cudaMemsetAsync(B.flags, 0, sizeof(int) * kFlagCount, st));
+    k_to32<<<dim3(nb(n, 256), n), 256, 0, st>>>(n, src, nullptr, B.LU32);
+    check_launch("k_to32");
     D4_CUDA_OK(cudaMemsetAsync(B.bar, 0, sizeof(unsigned) * 64, st));
     D4_CUDA_OK(cudaMemsetAsync(B.mask, 0, sizeof(unsigned) * c.lu_mask_words, st));
-    D4_CUDA_OK(cudaMemcpyAsync(B.LU32, A, bytes, cudaMemcpyDeviceToDevice, st));
-    if (copy_matrix) D4_CUDA_OK(cudaMemcpyAsync(B.A32, A, bytes, cudaMemcpyDeviceToDevice, st));
-    if (after_copy) D4_CUDA_OK(cudaEventRecord(after_copy, st));
     coop::CoopArgs<float> a;
     a.n = n;
     a.A = B.LU32;
@@ -438,8 +246,15 @@ void factor32_async(Ctx &c, const Mix32Bufs &B, const float *A, bool copy_matrix
     check_launch("k_lu_coop<float>");
 }
 
+// After a pivoted factorisation into the primary buffers: its row permutation
+// becomes the block LU's static pivots.
+void adopt_pivots(Ctx &c) {
+    D4_CUDA_OK(cudaMemcpyAsync(c.spiv, c.perm, sizeof(int) * c.n, cudaMemcpyDeviceToDevice,
+                               c.stream));
+}
+
 int factor32(Ctx &c) {
-    factor32_async(c, primary_mix32(c), c.A32, false, c.lu32_grid, c.stream, nullptr);
+    factor32_async(c, primary_mix32(c), c.A, false, c.lu32_grid, c.stream, nullptr);
     D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
                                cudaMemcpyDeviceToHost, c.stream));
     D4_CUDA_OK(cudaStreamSynchronize(c.stream));
@@ -449,12 +264,13 @@ int factor32(Ctx &c) {
         ++c.m_fallbacks;
         c.m_fast = 0;
         try {
-            factor32_async(c, primary_mix32(c), c.A32, false, c.lu32_grid, c.stream, nullptr);
+            factor32_async(c, primary_mix32(c), c.A, false, c.lu32_grid, c.stream, nullptr);
         } catch (...) {
             c.m_fast = 1;
             throw;
         }
         c.m_fast = 1;
+        adopt_pivots(c);
         D4_CUDA_OK(cudaMemcpyAsync(c.h_flags, c.flags, sizeof(int) * kFlagCount,
                                    cudaMemcpyDeviceToHost, c.stream));
         D4_CUDA_OK(cudaStreamSynchronize(c.stream));
@@ -480,11 +296,14 @@ int coop_grid_size32(int n) {
 }
 
 // FP32 solve with B's factors: LU32^-1 r (r FP64 in, result FP32), by the
-// block solves of the block LU, or by the cluster solve of the pivoted LU.
-// Returns the result's buffer.
-static const float *solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const double *r) {
+// block solves of the block LU (rows of r through the static pivots), or by
+// the cluster solve of the pivoted LU.  Sweep `it` of the refinement: the
+// block solve returns at once when sweep it - 1 converged.  Returns the
+// result's buffer.
+static const float *solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const double *r,
+                                 int it) {
     if (*B.blk) {
-        blu_solve_async(B.blu, c.n, B.LU32, r, B.flags, st);
+        blu_solve_async(B.blu, c.n, B.LU32, r, c.spiv, B.conv, it, B.flags, st);
         return B.blu.xs;
     }
     trsv::GArgs g{};
@@ -495,20 +314,28 @@ static const float *solve32_once(Ctx &c, const Mix32Bufs &B, cudaStream_t st, co
     return B.c32;
 }
 
-// The refinement loop: c = LU32^-1 r, dx += c, r = g - A32 dx, c.ir_iters
-// times from dx = 0, r = g (k_ir_init); dx alternates between B.dx and B.dx2.
-// Returns the buffer holding the final dx.
+// The refinement sweeps (k_ir_init has set dx = 0, r = g, conv[0] = max|g|):
+// c = LU32^-1 r, dx += c, r = g - A dx, until converged or kIrMax sweeps; dx
+// alternates between B.dx and B.dx2, and a converged sweep only carries it
+// over, so after kIrMax launches the buffer is known on the host.  Returns it.
 static const double *refine(Ctx &c, const Mix32Bufs &B, cudaStream_t st) {
     const int n = c.n, chunk = 256;
     double *dxa = B.dx, *dxb = B.dx2;
-    for (int it = 0; it < c.ir_iters; ++it) {
-        const float *corr = solve32_once(c, B, st, B.r);
+    for (int it = 0; it < kIrMax; ++it) {
+        const float *corr = solve32_once(c, B, st, B.r, it);
         k_resid_fused<<<dim3(nb(n, 256), nb(n, chunk)), 256, 0, st>>>(
-            n, B.A32, dxa, corr, dxb, B.g, B.part, chunk, nb(n, chunk), B.cnt, B.r);
+            n, B.A64, dxa, corr, dxb, B.g, B.part, chunk, nb(n, chunk), B.cnt, B.r, B.conv, it);
         check_launch("k_resid_fused");
         std::swap(dxa, dxb);
     }
     return dxa;
+}
+
+static void ir_start(Ctx &c, const Mix32Bufs &B, cudaStream_t st, const trsv::GArgs &ga) {
+    const int n = c.n;
+    D4_CUDA_OK(cudaMemsetAsync(B.conv, 0, sizeof(unsigned long long) * (kIrMax + 1), st));
+    k_ir_init<<<nb(n, 256), 256, 0, st>>>(n, ga, B.g, B.r, B.dx, B.conv);
+    check_launch("k_ir_init");
 }
 
 void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double *dx_out,
@@ -524,8 +351,7 @@ void solve_update32_with(Ctx &c, const Mix32Bufs &B, const double *dvec, double 
     ga.s_init = s_init;
     ga.x_new = x_new;
     ga.x_old = x_old;
-    k_ir_init<<<nb(n, 256), 256, 0, st>>>(n, ga, B.g, B.r, B.dx);
-    check_launch("k_ir_init");
+    ir_start(c, B, st, ga);
     const double *dx = refine(c, B, st);
     k_absmax2<<<64, 256, 0, st>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");
@@ -540,8 +366,7 @@ void solve_plain32(Ctx &c, const double *g) {
     trsv::GArgs ga{};
     ga.gmode = -1;
     ga.g_in = g;
-    k_ir_init<<<nb(n, 256), 256, 0, c.stream>>>(n, ga, B.g, B.r, B.dx);
-    check_launch("k_ir_init");
+    ir_start(c, B, c.stream, ga);
     const double *dx = refine(c, B, c.stream);
     k_absmax2<<<64, 256, 0, c.stream>>>(n, B.r, B.g, B.resid + 2 * *B.resid_count);
     check_launch("k_absmax2");

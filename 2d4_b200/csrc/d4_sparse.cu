@@ -372,16 +372,12 @@ void sparse_free(Ctx &c) {
         if (b) cudaFree(b);
 }
 
-// CSR of the current matrix (FP64 A, or the mixed form's FP32 A32).  Reads the
-// entry count back to size the index and value arrays (one host sync).
+// CSR of the current matrix (the FP64 A of either form).  Reads the entry
+// count back to size the index and value arrays (one host sync).
 void sparse_prepare(Ctx &c) {
     const int n = c.n;
-    const bool mixed = c.p.precision == D4_PREC_MIXED;
     const dim3 grid(sp::nb(n, 128), c.sp_nch);
-    if (mixed)
-        sp::k_csr_count<float><<<grid, 128, 0, c.stream>>>(n, c.A32, c.sp_cnt);
-    else
-        sp::k_csr_count<double><<<grid, 128, 0, c.stream>>>(n, c.A, c.sp_cnt);
+    sp::k_csr_count<double><<<grid, 128, 0, c.stream>>>(n, c.A, c.sp_cnt);
     check_launch("k_csr_count");
     sp::k_csr_rows<<<1, 1024, 0, c.stream>>>(n, c.sp_nch, c.sp_cnt, c.sp_off, c.sp_rp);
     check_launch("k_csr_rows");
@@ -399,12 +395,8 @@ void sparse_prepare(Ctx &c) {
         D4_CUDA_OK(d4::dmalloc((void **)&c.sp_val, sizeof(double) * (size_t)c.sp_cap));
     }
     c.sp_nnz = nnz;
-    if (mixed)
-        sp::k_csr_fill<float><<<grid, 128, 0, c.stream>>>(n, c.A32, c.sp_off, c.sp_rp, c.sp_ci,
-                                                          c.sp_val, c.sp_dinv);
-    else
-        sp::k_csr_fill<double><<<grid, 128, 0, c.stream>>>(n, c.A, c.sp_off, c.sp_rp, c.sp_ci,
-                                                           c.sp_val, c.sp_dinv);
+    sp::k_csr_fill<double><<<grid, 128, 0, c.stream>>>(n, c.A, c.sp_off, c.sp_rp, c.sp_ci,
+                                                       c.sp_val, c.sp_dinv);
     check_launch("k_csr_fill");
     c.sp_dense_ready = 0;
 }

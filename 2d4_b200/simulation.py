@@ -422,17 +422,13 @@ class Simulation:
 class Field:
     """Field::xy / Field::xy_diff_x (src/Fields/Field.cpp:333-346) evaluated on
     the device in FP64; with tabulated=True, the tabulated field
-    (PeriodicShearStressELTE's role, table_size intervals per axis); with
-    mixed=True, the mixed form's field (the FP64 stress and the FP32
-    compensated gradient)."""
+    (PeriodicShearStressELTE's role, table_size intervals per axis)."""
 
-    def __init__(self, device=0, tabulated=False, table_size=1024, mixed=False):
+    def __init__(self, device=0, tabulated=False, table_size=1024):
         self.lib = _lib.load()
         p = _lib.Params()
         self.lib.d4_default_params(C.byref(p))
         p.device = device
-        if mixed:  # the mixed form's field: FP64 stress, FP32 gradient
-            p.precision = _lib.D4_PREC_MIXED
         if tabulated:
             p.field = _lib.D4_FIELD_TABULATED
             p.table_size = table_size

@@ -47,7 +47,8 @@ enum {
 /* Arithmetic of the hot path. */
 enum {
     D4_PREC_FP64 = 0,  /* plain form: FP64 throughout, reference operation order */
-    D4_PREC_MIXED = 1  /* FP32 pair sums + TF32 tensor-core LU + FP64 refinement */
+    D4_PREC_MIXED = 1  /* FP64 sweeps and matrix; FP32 tensor-core LU and solves inside
+                          FP64 iterative refinement */
 };
 
 /* Linear solver of the implicit step.  The reference factorises the (cutoff-
@@ -188,12 +189,12 @@ int d4_jacobian(void *ctx, const double *x, const double *y, double stepsize, do
 int d4_jacobian_from_prev(void *ctx, double factor, double *a_colmajor, double *dvec);
 
 /* Replace the device matrix by a dense column-major n x n matrix (the
- * umfpack_di_numeric input of src/simulation.cpp:638, expanded from CSC).  The
- * mixed form stores it rounded to FP32. */
+ * umfpack_di_numeric input of src/simulation.cpp:638, expanded from CSC). */
 int d4_set_matrix(void *ctx, const double *a_colmajor);
 
 /* Factorise the device Jacobian.  Returns D4_WARN_SINGULAR on an exact zero
- * pivot, like umfpack_di_numeric.  Mixed form: the block LU, or the pivoted
+ * pivot, like umfpack_di_numeric.  Mixed form: its FP32 rounding, by the block
+ * LU (rows in the order of the last pivoted factorisation), or by the pivoted
  * FP32 LU when a diagonal tile met a zero or non-finite pivot. */
 int d4_factor(void *ctx);
 
@@ -201,7 +202,8 @@ int d4_factor(void *ctx);
  * D4_WARN_SINGULAR like umfpack_di_solve and, like it, leaves the result as
  * computed; d4_attempt/d4_run apply solveEQSys's zeroing of entries outside
  * (-1, 1) (src/simulation.cpp:646-658) themselves.  Mixed form: the FP32
- * factors' solve refined in FP64 against the FP32 matrix. */
+ * factors' solves refined in FP64 against the FP64 matrix (at most 4 sweeps,
+ * stopping at max|g - A dx| <= 1e-12 max|g|). */
 int d4_solve(void *ctx, const double *g, double *dx);
 
 /* Reset the per-dislocation tolerances (PrecisionHandler::reset). */
@@ -389,9 +391,7 @@ int d4_speeds_noalloc(int n, const double *x, const double *y, double ext_stress
                       double *tol, double min_prec_sq, void *stream);
 
 /* Single field evaluations on the device, for checks: the context's field
- * (analytic FP64 Field::xy / Field::xy_diff_x, or the tabulated field; in the
- * mixed form the FP64 stress its speeds use and the FP32 compensated gradient
- * its matrix uses). */
+ * (analytic FP64 Field::xy / Field::xy_diff_x, or the tabulated field). */
 int d4_field_eval(void *ctx, int count, const double *dx, const double *dy, double *xy,
                   double *xy_diff_x);
 

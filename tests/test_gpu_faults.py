@@ -5,7 +5,7 @@ build, dumps state on non-finite values (src/simulation.cpp:754-948); without
 those checks a NaN error ratio fails every attempt while getNewStepSize
 doubles h forever.  Here:
   - d4_set_positions rejects non-finite and out-of-cell positions (D4_ERR_ARG);
-  - a step whose error ratio is not finite (a step size so large that the
+  - a step whose error ratio is not finite (an infinite step size, so that the
     Jacobian overflows) ends d4_advance with D4_ERR_STATE instead of looping;
   - every bounded device wait gives up after its limit and reports
     D4_ERR_STATE through the host (d4_wait_selftest runs the cooperative LU's
@@ -61,7 +61,10 @@ def test_set_positions_rejects_bad_values(pkg):
 def test_nonfinite_ratio_stops_the_loop(pkg, mixed):
     mode = pkg._lib.D4_PREC_MIXED if mixed else pkg._lib.D4_PREC_FP64
     e, x, y = make_engine(pkg, 256 if mixed else 64, 1000, mode)
-    e._call("d4_set_time", C.c_double(0.0), C.c_double(1e300))
+    # an infinite step size: the Jacobian and residuals overflow, the positions
+    # and the error ratio become NaN (a large finite h is no test: the implicit
+    # step's displacement stays finite)
+    e._call("d4_set_time", C.c_double(0.0), C.c_double(float("inf")))
     r = pkg._lib.RunResult()
     st = e.lib.d4_advance(e.ctx, C.c_longlong(1), C.byref(r))
     assert st == pkg._lib.D4_ERR_STATE

@@ -1,13 +1,12 @@
-"""GPU checks of the mixed-precision form against the FP64 oracle (marked gpu).
+"""GPU checks of the mixed-precision form (marked gpu).
 
-FP32 pair gradient with compensated image sums and FP32 Jacobian, block LU on
-the tensor cores; FP64 speeds (the residual's pair stress), residuals,
-refinement, positions and acceptance.  Tolerances: the speeds to 1e-12
-relative (FP64 field, pair sums in another order than the reference's); the
-matrix to per-pair FP32 rounding (~1e-7 relative); the refined solve to 1e-10
-relative residual; one attempt's positions to 1e-10; 1000 accepted steps of the
-headline workload to 1e-8 against the plain FP64 form along the same step
-sequence, the bound the mixed form is built to.
+The mixed form keeps the FP64 form's sweeps, matrix, residuals, updates and
+step control, and runs the factorisations and triangular solves in FP32 (the
+block LU on the tensor cores) inside FP64 iterative refinement against the
+FP64 matrix.  Tolerances: the speeds and the matrix to 1e-12 relative of the
+oracle's (they are the FP64 form's); one attempt's positions to 1e-10; 1000
+accepted steps of the headline workload to 1e-8 against the plain FP64 form
+along the same step sequence, the bound the mixed form is built to.
 """
 import numpy as np
 import pytest
@@ -57,8 +56,8 @@ def test_mixed_jacobian(pkg, restated):
     p = restated.params()
     mps, _, cut, cs = restated.derived(p, n)
     vao, vbo, ao, do = restated.jacobian(x, y, 1e-4, 0.0, 0.0, cs, cut)
-    assert np.abs(a - ao).max() / np.abs(ao).max() < 2e-6
-    assert np.abs(d - do).max() < 1e-6
+    assert np.abs(a - ao).max() / np.abs(ao).max() < 1e-12
+    assert np.abs(d - do).max() < 1e-12
 
 
 @pytest.mark.parametrize("n,h", [(256, 5e-7), (1024, 2e-7)])
@@ -98,7 +97,7 @@ def test_mixed_fixed_steps_vs_fp64(pkg):
     assert out[0][1].attempts == out[1][1].attempts
     assert out[0][1].failed_steps == out[1][1].failed_steps
     d, _, _, _ = pkg.dconf.conf_compare(out[1][0], y, out[0][0], y)
-    assert d < 1e-7
+    assert d < 1e-9
 
 
 def test_mixed_1000_steps_vs_fp64(pkg):
@@ -129,33 +128,3 @@ def test_mixed_1000_steps_vs_fp64(pkg):
     assert st["block_factorizations"] > 0 and st["worst_refined_residual"] < 1e-9
     for e in engs:
         e.close()
-
-
-def test_mixed_field_error_budget_vs_ieee(pkg, golden):
-    """The FP32 compensated gradient (the matrix's field) against the exact
-    truncated image sum, the reference's IEEE variant (src/Fields/Field.cpp:
-    26-168, from its own evaluator: golden_runs.npz ieee_*), on the field grid.
-    The reference's default formula differs from the IEEE sum by up to ~3e-4
-    relative in the gradient (its precision study,
-    sandbox/ieee_hyperbolic/README.md:40-43); the FP32 form adds at most FP32
-    rounding of the image sum on top: its error against the IEEE sum stays
-    within the default formula's error plus 2e-5 of the gradient's scale, and
-    its median relative error below 1e-5.  The FP64 stress (the residual's
-    field) matches the IEEE sum as closely as the reference's default formula."""
-    import os
-    gr = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
-                              "golden_runs.npz"))
-    fx, fy = golden["field_dx"], golden["field_dy"]
-    f = pkg.Field(mixed=True)
-    xy, xyd = f.eval(fx, fy)
-    ieee_s, ieee_g = gr["ieee_xy"], gr["ieee_xyd"]
-    ref_s, ref_g = golden["field_xy"], golden["field_xyd"]
-    m = np.abs(ieee_g) > 1e-3
-    err32 = np.abs(xyd[m] - ieee_g[m])
-    err_ref = np.abs(ref_g[m] - ieee_g[m])
-    scale = np.abs(ieee_g[m])
-    assert np.all(err32 <= err_ref + 2e-5 * scale)
-    assert np.median(err32 / scale) < 1e-5
-    ms = np.abs(ieee_s) > 1e-3
-    assert np.all(np.abs(xy[ms] - ieee_s[ms]) <= np.abs(ref_s[ms] - ieee_s[ms]) +
-                  1e-12 * np.abs(ieee_s[ms]))
