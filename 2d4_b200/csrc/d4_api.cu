@@ -191,6 +191,10 @@ void read_async_errors(Ctx &c) {
     check_async_errors(c);
 }
 
+// Mixed form: attempts run on the FP64 path after a fallback before the block
+// LU is tried again.
+constexpr int kSkipAfterFallback = 16;
+
 // Grid split of an attempt's two concurrent cooperative factorisations:
 // stage I's chain (one LU, two solves, one sweep) is the shorter one, so it
 // gets 40% of the co-resident CTAs and stage II's factorisation the rest.
@@ -343,6 +347,7 @@ static double worst_refined(const unsigned long long *rb) {
         double r, g;
         std::memcpy(&r, &rb[2 * k], 8);
         std::memcpy(&g, &rb[2 * k + 1], 8);
+        if (std::isnan(r) || std::isnan(g)) return NAN;  // a NaN must fail the checks
         if (g > 0) worst = std::max(worst, r / g);
     }
     return worst;
@@ -477,8 +482,10 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
 }
 
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
-static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
-    if (c.overlap) {
+// fp64: in the mixed form, run this attempt on the FP64 form's factorisations
+// and solves (sequentially: the second stream's buffers are the mixed form's).
+static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res, bool fp64 = false) {
+    if (c.overlap && !(fp64 && c.p.precision == D4_PREC_MIXED)) {
         int singular = 0;
         double refine = 0;
         if (c.p.precision == D4_PREC_MIXED)
@@ -500,7 +507,7 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
     const double t_1__ = t0 + h;
     const double t_1p2 = t0 + h / 2;
     int singular = 0, pivoted = 0;
-    const bool mixed = c.p.precision == D4_PREC_MIXED;
+    const bool mixed = c.p.precision == D4_PREC_MIXED && !fp64;
     auto jac = [&](const double *x, double hh, double ta, double tb, double *va, double *vb) {
         ProfScope ps(c, D4_CAT_JACOBIAN);
         d4::jacobian64(c, x, c.y, hh, ext_stress(pr, ta), ext_stress(pr, tb), va, vb);
@@ -595,22 +602,30 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res) {
 // above kRefineLimit, the attempt is redone with the pivoted cooperative LU,
 // so its result is that of the exact-pivoting path.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
-    if (c.p.precision != D4_PREC_MIXED || !c.m_fast) return attempt_once(c, t0, h, res);
+    if (c.p.precision != D4_PREC_MIXED) return attempt_once(c, t0, h, res);
+    if (!c.m_fast || c.m_skip > 0) {
+        // the FP64 form's attempt: block LU switched off, or a recent fallback
+        if (c.m_skip > 0) --c.m_skip;
+        ++c.m_fp64_attempts;
+        attempt_once(c, t0, h, res, true);
+        d4::adopt_pivots(c);
+        return D4_OK;
+    }
     const long long before = c.m_blocklu;
     attempt_once(c, t0, h, res);
     if (c.m_blocklu == before) return D4_OK;  // no dense factorisation ran (GMRES)
     const double rr = res->refine_residual;
-    if (!(rr <= c.m_worst_refine)) c.m_worst_refine = rr;
-    if (!res->singular && rr <= d4::kRefineLimit) return D4_OK;
-    ++c.m_fallbacks;
-    c.m_fast = 0;
-    try {
-        attempt_once(c, t0, h, res);
-    } catch (...) {
-        c.m_fast = 1;
-        throw;
+    if (!res->singular && rr <= d4::kRefineLimit) {
+        if (rr > c.m_worst_refine) c.m_worst_refine = rr;
+        return D4_OK;
     }
-    c.m_fast = 1;
+    // the refinement did not converge (the Jacobian too ill-conditioned for FP32
+    // factors) or a diagonal tile met a bad pivot: the FP64 form's attempt, and
+    // the next kSkipAfterFallback attempts go there directly
+    ++c.m_fallbacks;
+    ++c.m_fp64_attempts;
+    c.m_skip = kSkipAfterFallback;
+    attempt_once(c, t0, h, res, true);
     d4::adopt_pivots(c);  // the next block LUs factorise P A with this attempt's P
     return D4_OK;
 }
@@ -740,7 +755,7 @@ int d4_create(void **out, int n, const d4_params *p) {
         // both forms: the FP64 matrix and pair-force scratch of the FP64 sweeps;
         // the FP64 factors only in the FP64 form
         dalloc(&c->A, nn);
-        dalloc(&c->LU, mixed ? 1 : nn);
+        dalloc(&c->LU, nn);  // the mixed form's FP64 attempts factorise here too
         dalloc(&c->F, nn);
         if (mixed) {
             dalloc(&c->A32, nn);
@@ -1324,11 +1339,13 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
 }
 
 int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
-                   double *worst_refined) {
+                   long long *fp64_attempts, double *worst_refined) {
     Ctx *c = (Ctx *)ctx;
-    if (!c || !block_factorizations || !fallbacks || !worst_refined) return D4_ERR_ARG;
+    if (!c || !block_factorizations || !fallbacks || !fp64_attempts || !worst_refined)
+        return D4_ERR_ARG;
     *block_factorizations = c->m_blocklu;
     *fallbacks = c->m_fallbacks;
+    *fp64_attempts = c->m_fp64_attempts;
     *worst_refined = c->m_worst_refine;
     return D4_OK;
 }

@@ -187,11 +187,15 @@ __device__ bool gauss_jordan(float *Sp, float *cbuf, float *rbuf) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) a[i][j] = Sp[(8 * tr + i) * kSp + 8 * tc + j];
     bool ok = true;
+    // pivots in groups of 8: the group index kb is a loop variable, the pivot's
+    // place kl inside the group is a compile-time index into the registers
+#pragma unroll 1
+    for (int kb = 0; kb < kB / 8; ++kb)
 #pragma unroll
-    for (int k = 0; k < kB; ++k) {
-        const int kb = k >> 3, kl = k & 7;
-        float *cb = cbuf + (k & 1) * kB;
-        float *rb = rbuf + (k & 1) * kB;
+    for (int kl = 0; kl < 8; ++kl) {
+        const int k = 8 * kb + kl;
+        float *cb = cbuf + (kl & 1) * kB;
+        float *rb = rbuf + (kl & 1) * kB;
         if (tc == kb) {
 #pragma unroll
             for (int i = 0; i < 8; ++i) cb[8 * tr + i] = a[i][kl];

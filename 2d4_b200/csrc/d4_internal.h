@@ -164,13 +164,14 @@ struct Ctx {
     int ir_iters = 2;
     // block LU path of the mixed form (d4_blu32.cu): on by default; an attempt
     // whose block factorisation met a bad pivot, or whose refined residual
-    // stayed above kRefineLimit, is redone with the pivoted cooperative LU
+    // stayed above kRefineLimit, is redone on the FP64 form's path
     int m_fast = 1;
     int *blu_tasks = nullptr;
     BluBufs blu;  // the primary buffer set's block-LU buffers
     BluState blu_state, blu_state_b;
     int m_blk = 0, m_blk_b = 0;  // Mix32Bufs::blk of the primary and stage-I buffer sets
-    long long m_blocklu = 0, m_fallbacks = 0;
+    long long m_blocklu = 0, m_fallbacks = 0, m_fp64_attempts = 0;
+    int m_skip = 0;  // attempts left on the FP64 path after a fallback
     double m_worst_refine = 0;
 
     // cutoff sparse path: CSR of the matrix and the GMRES work space

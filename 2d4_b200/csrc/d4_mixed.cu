@@ -47,16 +47,21 @@ __device__ __forceinline__ unsigned long long obits(double v) {
     return (unsigned long long)__double_as_longlong(v);  // ordered for v >= 0
 }
 
-// max over the block of v (>= 0) into *out by atomicMax on the bit pattern.
+// max of two non-negative values where a NaN wins (fmax would drop it): a NaN
+// residual must fail the convergence and fallback checks.
+__device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+// max over the block of v (>= 0 or NaN) into *out by atomicMax on the bit
+// pattern (a NaN's bits exceed every finite value's).
 __device__ void block_absmax(double v, unsigned long long *out) {
     __shared__ double wm[8];
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
     if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wm[w]);
-        atomicMax(out, obits(m));
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = nanmax(m, wm[w]);
+        atomicMax(out, obits(fabs(m)));
     }
 }
 
@@ -143,16 +148,16 @@ __global__ void __launch_bounds__(256) k_resid_fused(int n, const double *__rest
 __global__ void k_absmax2(int n, const double *r, const double *g, unsigned long long *out) {
     double m1 = 0, m2 = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        m1 = fmax(m1, fabs(r[i]));
-        m2 = fmax(m2, fabs(g[i]));
+        m1 = nanmax(m1, fabs(r[i]));
+        m2 = nanmax(m2, fabs(g[i]));
     }
     for (int o = 16; o > 0; o >>= 1) {
-        m1 = fmax(m1, __shfl_down_sync(0xffffffffu, m1, o));
-        m2 = fmax(m2, __shfl_down_sync(0xffffffffu, m2, o));
+        m1 = nanmax(m1, __shfl_down_sync(0xffffffffu, m1, o));
+        m2 = nanmax(m2, __shfl_down_sync(0xffffffffu, m2, o));
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicMax(out, obits(m1));
-        atomicMax(out + 1, obits(m2));
+        atomicMax(out, obits(fabs(m1)));
+        atomicMax(out + 1, obits(fabs(m2)));
     }
 }
 

@@ -282,14 +282,20 @@ __device__ __forceinline__ void error_ratio_block(int n, const double *xb, const
     __shared__ int si[32];
     double best = 0;
     int bi = -1;
+    int bad = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double e = fabs(xb[i] - x2[i]);
         double t = use_dipole ? e * e / tol[i] : e * e / min_prec_sq;
+        bad |= !isfinite(e);
         if (t > best) {
             best = t;
             bi = i;
         }
     }
+    // the reference's maximum skips a NaN (src/simulation.cpp:692-700); a
+    // position that is not finite makes the ratio NaN here, which the host
+    // turns into an error instead of a step
+    bad = __syncthreads_or(bad);
     for (int o = 16; o > 0; o >>= 1) {
         double ov = __shfl_down_sync(0xffffffffu, best, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
@@ -317,7 +323,7 @@ __device__ __forceinline__ void error_ratio_block(int n, const double *xb, const
             }
         }
         if (l == 0) {
-            out[0] = best;
+            out[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : best;
             out[1] = bi;
         }
     }

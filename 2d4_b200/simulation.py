@@ -351,16 +351,16 @@ class Engine:
 
     def mixed_stats(self):
         """Mixed form's factorisations (d4_mixed_stats): block LUs run, attempts
-        redone with the pivoted LU, worst refined residual of the block-LU
-        attempts."""
-        b, f, w = C.c_longlong(), C.c_longlong(), C.c_double()
-        self._call("d4_mixed_stats", C.byref(b), C.byref(f), C.byref(w))
+        redone on the FP64 path, attempts on the FP64 path in all, worst refined
+        residual of the block-LU attempts that stood."""
+        b, f, a, w = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_double()
+        self._call("d4_mixed_stats", C.byref(b), C.byref(f), C.byref(a), C.byref(w))
         return {"block_factorizations": b.value, "fallbacks": f.value,
-                "worst_refined_residual": w.value}
+                "fp64_attempts": a.value, "worst_refined_residual": w.value}
 
     def set_block_lu(self, enable=True):
-        """Mixed form: block LU with per-attempt fallback (default), or always
-        the pivoted cooperative LU (d4_set_block_lu)."""
+        """Mixed form: block LU with per-attempt fallback (default), or every
+        attempt on the FP64 form's factorisations and solves (d4_set_block_lu)."""
         self._call("d4_set_block_lu", int(bool(enable)))
 
     def positions(self):

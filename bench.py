@@ -393,7 +393,8 @@ def mixed_vs_fp64(pkg, n, seed, tau, steps, start=None, report_every=100):
             "speedup": t[0] / t[1], "same_steps": same, "attempts": att, "failed": fail,
             "max_position_diff_vs_fp64": worst, "position_diff_every_%d_steps" % report_every: errs,
             "mixed_block_factorizations": ms["block_factorizations"],
-            "mixed_fallbacks_to_pivoted_lu": ms["fallbacks"],
+            "mixed_fallbacks_to_fp64": ms["fallbacks"],
+            "mixed_fp64_path_attempts": ms["fp64_attempts"],
             "mixed_worst_refined_residual": ms["worst_refined_residual"],
             "fp64_ms_per_call": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof["fp64"].items()},
             "mixed_ms_per_call": {k: round(v[0] / max(v[1], 1), 4)

@@ -249,12 +249,19 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
 
 /* Mixed form's factorisations (no counterpart in the reference): block LU
  * factorisations run (128 x 128 tiles on the tensor cores, no row interchanges
- * between tiles), attempts redone with the pivoted cooperative LU because a
- * diagonal tile met a zero or non-finite pivot or a refined residual stayed
- * above 1e-9 (max|g - A dx| / max|g|), and the worst refined residual of the
- * block-LU attempts. */
+ * between tiles, rows in the order of the last FP64 factorisation), attempts
+ * redone on the FP64 form's path because a diagonal tile met a zero or
+ * non-finite pivot or the refinement left max|g - A dx| above 1e-9 max|g| (the
+ * Jacobian too ill-conditioned for FP32 factors), attempts that ran on the FP64
+ * path in all (the redone ones and the 16 after each), and the worst refined
+ * residual of the block-LU attempts that stood. */
 int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
-                   double *worst_refined);
+                   long long *fp64_attempts, double *worst_refined);
+
+/* Mixed form: enable = 1 (the default) runs attempts on the block LU with the
+ * fallback that d4_mixed_stats describes; 0 runs every attempt on the FP64
+ * form's factorisations and solves.  No counterpart in the reference. */
+int d4_set_block_lu(void *ctx, int enable);
 
 /* Pair-tile autotuner (no counterpart in the reference): the FP64 form's pair
  * kernels evaluate each 32 x 32 tile of pairs with 32 x threads_y threads;
