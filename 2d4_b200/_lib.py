@@ -79,6 +79,8 @@ SIGNATURES = {
     "d4_factor": (C.c_int, [_vp]),
     "d4_solve": (C.c_int, [_vp, _dp, _dp]),
     "d4_reset_tolerance": (C.c_int, [_vp]),
+    "d4_get_tolerance": (C.c_int, [_vp, _dp]),
+    "d4_set_tolerance": (C.c_int, [_vp, _dp]),
     "d4_attempt": (C.c_int, [_vp, C.c_double, C.c_double, C.POINTER(AttemptResult)]),
     "d4_get_attempt": (C.c_int, [_vp, _dp, _dp, _dp]),
     "d4_run": (C.c_int, [_vp, C.POINTER(RunIO), C.POINTER(RunResult)]),

@@ -937,6 +937,31 @@ int d4_reset_tolerance(void *ctx) {
     D4_GUARD_END(c)
 }
 
+int d4_get_tolerance(void *ctx, double *tol) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !tol) return D4_ERR_ARG;
+    D4_GUARD_BEGIN
+    download(*c, tol, c->tol);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
+int d4_set_tolerance(void *ctx, const double *tol) {
+    Ctx *c = (Ctx *)ctx;
+    if (!c || !tol) return D4_ERR_ARG;
+    for (int i = 0; i < c->n; ++i)
+        if (!(std::isfinite(tol[i]) && tol[i] >= 0))
+            return fail(c, D4_ERR_ARG,
+                        "d4_set_tolerance: entry " + std::to_string(i) +
+                            " is not a finite non-negative number");
+    D4_GUARD_BEGIN
+    upload(*c, c->tol, tol);
+    sync(*c);
+    return D4_OK;
+    D4_GUARD_END(c)
+}
+
 int d4_speeds(void *ctx, const double *x, const double *y, double sim_time, double *v,
               double *tol) {
     Ctx *c = (Ctx *)ctx;
@@ -1232,7 +1257,7 @@ int d4_run(void *ctx, const d4_run_io *io, d4_run_result *res) {
         if (!log) return fail(c, D4_ERR_IO, std::string("cannot open log ") + io->log_path);
         log << std::scientific << std::setprecision(16);
     }
-    if (c->p.precision == D4_PREC_FP64) d4::autotune_pairs(*c);
+    d4::autotune_pairs(*c);  // both forms run the FP64 pair kernels
     start_state(c);
     c->rs.wall_start = c->rs.wall_last = wall_time();
     const d4::RunState before = c->rs;
@@ -1267,7 +1292,7 @@ int d4_advance(void *ctx, long long accepted_steps, d4_run_result *res) {
     Ctx *c = (Ctx *)ctx;
     if (!c || accepted_steps < 0) return D4_ERR_ARG;
     D4_GUARD_BEGIN
-    if (c->p.precision == D4_PREC_FP64) d4::autotune_pairs(*c);
+    d4::autotune_pairs(*c);  // both forms run the FP64 pair kernels
     if (!c->rs.started) {
         start_state(c);
         // the first attempt's tolerances include the initial sweep of run()

@@ -14,12 +14,14 @@ constexpr int NB = 32;
 constexpr int kThreads = 256;
 constexpr long long kSpinLimit = 1ll << 24;  // x >= 64 ns each: > 1 s
 constexpr int kGenWord = 32;
-// Dynamic shared memory: the rows-below buffer, and for the FP32 form the four
+// Dynamic shared memory: the narrow last block's rows (a row of NB + 1 entries
+// per thread, also the trailing update's second piece buffer), the diagonal
+// block's pre-division values (NB rows), and for the FP32 form after them the four
 // tensor-core operand tiles (L21 and U12 as TF32 hi and lo parts, 16 KiB each,
 // 1 KiB aligned) plus the MMA completion barrier and the TMEM address slot.
 constexpr size_t kOpTileBytes = 128 * NB * 4;
 template <typename T>
-__host__ __device__ constexpr size_t kRowBufRaw() { return sizeof(T) * kThreads * (NB + 1); }
+__host__ __device__ constexpr size_t kRowBufRaw() { return sizeof(T) * (kThreads + NB) * (NB + 1); }
 template <typename T>
 __host__ __device__ constexpr size_t kTcOffset() { return (kRowBufRaw<T>() + 1023) / 1024 * 1024; }
 template <typename T>
@@ -93,14 +95,16 @@ __device__ __forceinline__ int src_row(int r, const int *sa, const int *sb, int 
 }
 
 // Diagonal block of the pass, in every CTA, by all its threads on shared
-// memory (two block barriers per column).  Pre-division values go to Q (CTA
-// 0), flags into the returned mask (meaningful in thread 0's and the column
-// owners' copies; they are OR-ed over the CTA).  A spare thread stores each
-// pivot's correctly rounded reciprocal in rs, for the rows below.
+// memory (two block barriers per column).  Pre-division values are kept in
+// qbuf and go to Q after the loop (CTA 0), so no block barrier waits for a
+// global store; flags go into the returned mask (meaningful in thread 0's and
+// the column owners' copies; they are OR-ed over the CTA).  A spare thread
+// stores each pivot's correctly rounded reciprocal in rs, for the rows below.
 template <typename T>
 __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[NB + 1],
-                                            T *rs, int k0, int kw, const int *sa, const int *sb,
-                                            int ns, unsigned skip, bool write_q) {
+                                            T *rs, T (*qbuf)[NB + 1], int k0, int kw,
+                                            const int *sa, const int *sb, int ns, unsigned skip,
+                                            bool write_q) {
     const int n = a.n;
     const int tid = threadIdx.x;
     unsigned msk = 0;
@@ -117,7 +121,7 @@ __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[N
         if (tid == NB) rs[k] = qdiv::recip(d);
         if (tid < NB) {
             const int r = tid;
-            if (write_q && r >= k && r < kw) Q[(size_t)(k0 + r) + (size_t)k * n] = s[r][k];
+            if (write_q && r >= k && r < kw) qbuf[r][k] = s[r][k];
             if (!sk) {
                 if (r == 0 && d == 0.0) msk |= 1u << k;
                 if (r > k && r < kw) {
@@ -139,6 +143,11 @@ __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[N
         }
         __syncthreads();
     }
+    if (write_q)
+        for (int t = tid; t < NB * NB; t += kThreads) {
+            const int r = t % NB, k = t / NB;
+            if (r >= k && r < kw && k < kw) Q[(size_t)(k0 + r) + (size_t)k * n] = qbuf[r][k];
+        }
     return msk;
 }
 
@@ -251,6 +260,131 @@ __device__ __noinline__ unsigned rows_below(const CoopArgs<T> &a, T *Q,
 }
 
 
+// The block's row swaps on every other column, then U12 = L11^-1 A12 on the
+// columns right of the block, a warp per column: lane r holds row r, column
+// k's value reaches the lanes below by shuffle (u_kj == 0 skips its updates,
+// as the oracle does).
+template <typename T>
+__device__ __noinline__ void finish_cols(const CoopArgs<T> &a, const T (*s)[NB + 1], int k0,
+                                         int kw, const int *sa, const int *sb, int ns) {
+    const int n = a.n, G = gridDim.x, cta = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    {
+        const int warps = G * (kThreads / 32);
+        for (int c = cta * (kThreads / 32) + warp; c < n - kw; c += warps) {
+            const int j = c < k0 ? c : c + kw;
+            T *cj = a.A + (size_t)j * n;
+            if (lane == 0) {
+                for (int t = 0; t < ns; ++t) {
+                    const T x = cj[sa[t]];
+                    cj[sa[t]] = cj[sb[t]];
+                    cj[sb[t]] = x;
+                }
+            }
+            __syncwarp();
+            if (j >= k0 + kw) {
+                T v = lane < kw ? cj[k0 + lane] : 0.0;
+                for (int k = 0; k < kw; ++k) {
+                    const T t = __shfl_sync(0xffffffffu, v, k);
+                    if (lane > k && lane < kw && t != 0.0) v = v - s[lane][k] * t;
+                }
+                if (lane < kw) cj[k0 + lane] = v;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+    // 8 bytes global -> shared without registers; zero-filled when !valid
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Trailing update A22 -= L21 U12 of the plain form, every entry in the
+// oracle's order (k ascending, product and difference rounded separately);
+// tiles holding the next block's columns also refresh P0.  64 x 64 tiles,
+// 4 x 4 entries per thread.  While a tile computes, the next tile's L21 and
+// U12 pieces stream into the other shared-memory buffer (cp.async) and its
+// entries into registers.
+template <typename T>
+__device__ __noinline__ void update_tiles(const CoopArgs<T> &a, int k0, int kw, T *buf0,
+                                          T *buf1) {
+    constexpr int kLd = 64 + 1;          // row stride of the L and U pieces
+    constexpr int kPiece = NB * kLd;     // one piece (L or U)
+    const int n = a.n, tid = threadIdx.x, cta = blockIdx.x, G = gridDim.x;
+    const int base = k0 + kw, rest = n - base;
+    const int tb = (rest + 63) / 64;
+    const int nk0 = base, nkw = min(NB, n - base);  // next block's columns
+    const int tr = tid % 16, tc = tid / 16;
+    const int ntiles = tb * tb;
+    T pa[4][4];
+    auto stage = [&](int tile, T *buf) {
+        const int i0 = base + (tile % tb) * 64, j0 = base + (tile / tb) * 64;
+        T *Ls = buf, *Us = buf + kPiece;
+#pragma unroll
+        for (int r = 0; r < 64 * NB / kThreads; ++r) {
+            const int t = tid + r * kThreads;
+            const int ii = t % 64, k = t / 64;
+            const bool vl = k < kw && i0 + ii < n;
+            cp_async8(Ls + k * kLd + ii, vl ? a.A + (size_t)(i0 + ii) + (size_t)(k0 + k) * n : a.A, vl);
+            const int k2 = t % NB, jj = t / NB;
+            const bool vu = k2 < kw && j0 + jj < n;
+            cp_async8(Us + k2 * kLd + jj, vu ? a.A + (size_t)(k0 + k2) + (size_t)(j0 + jj) * n : a.A, vu);
+        }
+        cp_async_commit();
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gi = i0 + tr + 16 * p, gj = j0 + tc + 16 * q;
+                pa[p][q] = (gi < n && gj < n) ? a.A[(size_t)gi + (size_t)gj * n] : T(0);
+            }
+    };
+    if (cta < ntiles) stage(cta, buf0);
+    int par = 0;
+    for (int tile = cta; tile < ntiles; tile += G, par ^= 1) {
+        const int i0 = base + (tile % tb) * 64, j0 = base + (tile / tb) * 64;
+        const T *Ls = par ? buf1 : buf0;
+        const T *Us = Ls + kPiece;
+        T acc[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] = pa[p][q];
+        cp_async_wait_all();
+        __syncthreads();  // this tile's pieces are in; the other buffer is free
+        if (tile + G < ntiles) stage(tile + G, par ? buf0 : buf1);
+#pragma unroll 2
+        for (int k = 0; k < kw; ++k) {
+            T lv[4], uv[4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) lv[p] = Ls[k * kLd + tr + 16 * p];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) uv[q] = Us[k * kLd + tc + 16 * q];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[p][q] = acc[p][q] - lv[p] * uv[q];
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gi = i0 + tr + 16 * p, gj = j0 + tc + 16 * q;
+                if (gi < n && gj < n) {
+                    a.A[(size_t)gi + (size_t)gj * n] = acc[p][q];
+                    if (gj >= nk0 && gj < nk0 + nkw)
+                        a.P0[(size_t)gi + (size_t)(gj - nk0) * n] = acc[p][q];
+                }
+            }
+        __syncthreads();  // the products are done with this buffer before it is refilled
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Tensor-core trailing update of the FP32 form (tcgen05, kind::tf32).
 //
@@ -346,11 +480,10 @@ __device__ __forceinline__ void fence_before() {
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     extern __shared__ __align__(16) unsigned char rowbuf_raw[];
-    T *rowbuf = reinterpret_cast<T *>(rowbuf_raw);  // kThreads rows of NB+1 entries
+    T *rowbuf = reinterpret_cast<T *>(rowbuf_raw);  // see kRowBufRaw
     __shared__ T s[NB][NB + 1];           // diagonal block (rows = positions k0..k0+31)
     __shared__ T rs[NB];                  // RN(1 / pivot) of the block's columns
-    __shared__ T Ls[NB][64 + 1];          // update: L21 tile
-    __shared__ T Us[NB][64 + 1];          // update: U12 tile
+    __shared__ __align__(16) T LUs[2 * NB * (64 + 1)];  // update: L21 and U12 pieces (buffer 0)
     __shared__ int sa[NB], sb[NB];        // swap list of the block (positions)
     __shared__ unsigned skip_mask;        // singular columns (skipped)
     __shared__ int ns_s;
@@ -412,8 +545,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             const int ns = ns_s;
             const unsigned skip = skip_mask;
             if (tid == 0) cta_mask = 0;
-            // diagonal block, redundantly in every CTA (warp 0), then the rows below
-            unsigned my_mask = diag_block(a, Q, s, rs, k0, kw, sa, sb, ns, skip, cta == 0);
+            // diagonal block, redundantly in every CTA, then the rows below
+            unsigned my_mask =
+                diag_block(a, Q, s, rs, reinterpret_cast<T (*)[NB + 1]>(rowbuf + kThreads * (NB + 1)),
+                           k0, kw, sa, sb, ns, skip, cta == 0);
             my_mask |= rows_below(a, Q, s, rs, rowbuf, k0, kw, sa, sb, ns, skip);
             if (my_mask) atomicOr(&cta_mask, my_mask);
             __syncthreads();
@@ -495,29 +630,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             }
         }
         // other columns: the block's swaps, then U12 = L11^-1 A12 (warp per column)
-        {
-            const int warps = G * (kThreads / 32);
-            for (int c = cta * (kThreads / 32) + warp; c < n - kw; c += warps) {
-                const int j = c < k0 ? c : c + kw;
-                T *cj = a.A + (size_t)j * n;
-                if (lane == 0) {
-                    for (int t = 0; t < ns; ++t) {
-                        const T x = cj[sa[t]];
-                        cj[sa[t]] = cj[sb[t]];
-                        cj[sb[t]] = x;
-                    }
-                }
-                __syncwarp();
-                if (j >= k0 + kw) {
-                    T v = lane < kw ? cj[k0 + lane] : 0.0;
-                    for (int k = 0; k < kw; ++k) {
-                        const T t = __shfl_sync(0xffffffffu, v, k);
-                        if (lane > k && lane < kw && t != 0.0) v = v - s[lane][k] * t;
-                    }
-                    if (lane < kw) cj[k0 + lane] = v;
-                }
-            }
-        }
+        finish_cols(a, s, k0, kw, sa, sb, ns);
         grid_barrier(a.bar, a.flags, gen, &dead_s);
         // ---------------------------------------------------------- update
         const int base = k0 + kw;
@@ -613,53 +726,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
                 __syncthreads();
             }
         } else if (rest > 0) {
-            const int tb = (rest + 63) / 64;
-            const int nk0 = base, nkw = min(NB, n - base);  // next block's columns
-            for (int tile = cta; tile < tb * tb; tile += G) {
-                const int i0 = base + (tile % tb) * 64, j0 = base + (tile / tb) * 64;
-                __syncthreads();
-                for (int t = tid; t < 64 * NB; t += kThreads) {
-                    const int ii = t % 64, k = t / 64;
-                    const int gi = i0 + ii;
-                    Ls[k][ii] = (k < kw && gi < n) ? a.A[(size_t)gi + (size_t)(k0 + k) * n] : T(0);
-                    const int k2 = t % NB, jj = t / NB;
-                    const int gj = j0 + jj;
-                    Us[k2][jj] =
-                        (k2 < kw && gj < n) ? a.A[(size_t)(k0 + k2) + (size_t)gj * n] : T(0);
-                }
-                __syncthreads();
-                const int tr = tid % 16, tc = tid / 16;
-                T acc[4][4];
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int gi = i0 + tr + 16 * p, gj = j0 + tc + 16 * q;
-                        acc[p][q] = (gi < n && gj < n) ? a.A[(size_t)gi + (size_t)gj * n] : T(0);
-                    }
-                for (int k = 0; k < kw; ++k) {
-                    T lv[4], uv[4];
-#pragma unroll
-                    for (int p = 0; p < 4; ++p) lv[p] = Ls[k][tr + 16 * p];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) uv[q] = Us[k][tc + 16 * q];
-#pragma unroll
-                    for (int p = 0; p < 4; ++p)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc[p][q] = acc[p][q] - lv[p] * uv[q];
-                }
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int gi = i0 + tr + 16 * p, gj = j0 + tc + 16 * q;
-                        if (gi < n && gj < n) {
-                            a.A[(size_t)gi + (size_t)gj * n] = acc[p][q];
-                            if (gj >= nk0 && gj < nk0 + nkw)
-                                a.P0[(size_t)gi + (size_t)(gj - nk0) * n] = acc[p][q];
-                        }
-                    }
-            }
+            update_tiles(a, k0, kw, LUs, rowbuf);  // buffer 1 reuses the panel's buffers
             // rows of the next block's columns above the trailing matrix are
             // never read from P0 (positions >= nk0 only)
         }

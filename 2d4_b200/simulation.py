@@ -251,6 +251,20 @@ class Engine:
     def reset_tolerance(self):
         self._call("d4_reset_tolerance")
 
+    def tolerance(self):
+        """The per-dislocation tolerances (squared distances)."""
+        t = np.empty(self.n)
+        self._call("d4_get_tolerance", _lib.ptr(t))
+        return t
+
+    def restore(self, x, y, sim_time, step_size, tol):
+        """Restarts the stepping loop from a saved state: positions, time,
+        step size and tolerances (the state carried between accepted steps)."""
+        x, y, tol = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, tol))
+        self._call("d4_set_positions", _lib.ptr(x), _lib.ptr(y))
+        self._call("d4_set_time", C.c_double(sim_time), C.c_double(step_size))
+        self._call("d4_set_tolerance", _lib.ptr(tol))
+
     def attempt(self, t0, h):
         r = _lib.AttemptResult()
         self._call("d4_attempt", C.c_double(t0), C.c_double(h), C.byref(r))

@@ -336,62 +336,87 @@ def attempt_roofline(prof, n, mixed, hbm_gbs, fp64_tf, tf32_tf):
     return r
 
 
-def mixed_vs_fp64(pkg, n, seed, tau, steps, start=None, report_every=100):
-    """The metric's comparison at one N: the plain FP64 form and the mixed form
-    from the same start, advanced in lockstep one accepted step at a time
-    (device time of each d4_advance by CUDA events), the max periodic
-    |x_mixed - x_fp64| after every step (the mixed form's error against the
-    FP64 form along the same step sequence: both forms must take the same
-    accepted/failed steps, reported as same_steps), and one profiled pass of
-    each form over the first steps for the per-call kernel times."""
+def mixed_vs_fp64(pkg, n, seed, tau, steps, start=None, free_steps=200, report_every=25):
+    """The mixed form against the plain FP64 form at one N.
+
+    Shadowed steps: the FP64 form takes `steps` accepted steps; before each
+    one the mixed form restarts from the FP64 form's state (positions, time,
+    step size, tolerances) and takes the same step.  Both are timed on the
+    device (CUDA events of each d4_advance), so the speed-up compares the same
+    accepted steps with the same step sizes, and the position difference after
+    each step is the mixed form's own error per step (max reported).
+
+    Free running: both forms, and the FP64 form started from positions moved
+    by 1e-15 (the dynamics' own sensitivity), advance `free_steps` accepted
+    steps independently; the differences to the FP64 form are reported side by
+    side every `report_every` steps.  One profiled pass of each form gives the
+    per-call kernel times."""
     if start is not None:
         x, y = start
     else:
         x, y, _ = pkg.dconf.generate_internal(n, seed)
-    engs = []
-    for mode in (pkg._lib.D4_PREC_FP64, pkg._lib.D4_PREC_MIXED):
+
+    def engine(mode, xx):
         sd = pkg.SimulationData()
-        sd.set_positions(x, y)
+        sd.set_positions(xx, y)
         sd.precision_mode = mode
         sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
-        engs.append(pkg.Engine(sd))
+        return pkg.Engine(sd)
+
+    F64, MIX = pkg._lib.D4_PREC_FP64, pkg._lib.D4_PREC_MIXED
+    f64, mix = engine(F64, x), engine(MIX, x)
+    mix.advance(0)
     t = [0.0, 0.0]
     att = [0, 0]
-    fail = [0, 0]
-    worst, errs = 0.0, []
-    same = True
-    for s in range(1, steps + 1):
-        for k, e in enumerate(engs):
-            r = e.advance(1)
-            t[k] += r.device_seconds
-            att[k] += int(r.attempts)
-            fail[k] += int(r.failed_steps)
-        same = same and att[0] == att[1]
-        d = pkg.dconf.conf_compare(engs[1].positions()[0], y, engs[0].positions()[0], y)[0]
+    same, worst = True, 0.0
+    for _ in range(steps):
+        x0, _ = f64.positions()
+        tol = f64.tolerance()
+        r0 = f64.advance(0)
+        mix.restore(x0, y, r0.sim_time, r0.step_size, tol)
+        r64 = f64.advance(1)
+        rmx = mix.advance(1)
+        t[0] += r64.device_seconds
+        t[1] += rmx.device_seconds
+        att[0] += int(r64.attempts)
+        att[1] += int(rmx.attempts)
+        same = same and r64.attempts == rmx.attempts
+        d = pkg.dconf.conf_compare(mix.positions()[0], y, f64.positions()[0], y)[0]
         worst = max(worst, d)
-        if s % report_every == 0 or s == steps:
-            errs.append([s, d])
-    ms = engs[1].mixed_stats()
-    for e in engs:
+    ms = mix.mixed_stats()
+    f64.close()
+    mix.close()
+
+    xp = x + 1e-15 * np.random.default_rng(5).standard_normal(n)
+    xp = np.where(xp >= 0.5, xp - 1.0, np.where(xp < -0.5, xp + 1.0, xp))
+    free = [engine(F64, x), engine(MIX, x), engine(F64, xp)]
+    curve = []
+    for s in range(1, free_steps + 1):
+        for e in free:
+            e.advance(1)
+        if s % report_every == 0:
+            ref = free[0].positions()[0]
+            curve.append([s, pkg.dconf.conf_compare(free[1].positions()[0], y, ref, y)[0],
+                          pkg.dconf.conf_compare(free[2].positions()[0], y, ref, y)[0]])
+    for e in free:
         e.close()
+
     # per-call kernel times: a profiled pass over a few steps from the same start
     prof = {}
-    for name, mode in (("fp64", pkg._lib.D4_PREC_FP64), ("mixed", pkg._lib.D4_PREC_MIXED)):
-        sd = pkg.SimulationData()
-        sd.set_positions(x, y)
-        sd.precision_mode = mode
-        sd.external_stress = pkg.FixedRateProtocol(tau, 0.0)
-        e = pkg.Engine(sd)
+    for name, mode in (("fp64", F64), ("mixed", MIX)):
+        e = engine(mode, x)
         e.advance(1)
         e.profile(True)
         e.advance(min(steps, 10))
         prof[name] = e.profile_read()
         e.close()
-    return {"n": n, "tau_ext": tau, "steps": steps,
+    return {"n": n, "tau_ext": tau, "shadowed_steps": steps,
             "fp64_dislocation_steps_per_s": n * steps / t[0],
             "mixed_dislocation_steps_per_s": n * steps / t[1],
-            "speedup": t[0] / t[1], "same_steps": same, "attempts": att, "failed": fail,
-            "max_position_diff_vs_fp64": worst, "position_diff_every_%d_steps" % report_every: errs,
+            "speedup": t[0] / t[1], "same_attempts": same, "attempts": att,
+            "max_position_error_per_step": worst,
+            "free_run_diff_vs_fp64": {"columns": ["step", "mixed", "fp64 from x0 + 1e-15"],
+                                      "rows": curve},
             "mixed_block_factorizations": ms["block_factorizations"],
             "mixed_fallbacks_to_fp64": ms["fallbacks"],
             "mixed_fp64_path_attempts": ms["fp64_attempts"],
@@ -608,8 +633,9 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed vs FP64 legs")
-    ap.add_argument("--mixed-steps", type=int, default=1000,
-                    help="accepted steps of the mixed vs FP64 legs (N=4096 and N=1024)")
+    ap.add_argument("--mixed-steps", type=int, default=0,
+                    help="shadowed accepted steps of the mixed vs FP64 legs (default: 200 at "
+                         "N=4096, 1000 at N=1024)")
     ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint,xpattern",
                     help="extra single-GPU legs (comma list, or 'none')")
     args = ap.parse_args()
@@ -745,11 +771,14 @@ def main():
                       "swaps_per_factorization": (lu1["swaps"] - lu0["swaps"]) / nlu}
     if ws == 1 and not args.no_mixed:
         tf32_tf = bf16 / 2
-        for key, kw in (("mixed_vs_fp64", dict(n=4096, seed=1002, tau=0.1)),
-                        ("mixed_vs_fp64_n1024", dict(n=1024, seed=1001, tau=0.05,
+        for key, kw in (("mixed_vs_fp64", dict(n=4096, seed=1002, tau=0.1, steps=200,
+                                               free_steps=100, report_every=10)),
+                        ("mixed_vs_fp64_n1024", dict(n=1024, seed=1001, tau=0.05, steps=1000,
                                                      start=start_state(pkg, WORKLOADS["c2"])))):
             try:
-                leg = mixed_vs_fp64(pkg, steps=args.mixed_steps, **kw)
+                if args.mixed_steps > 0:
+                    kw["steps"] = args.mixed_steps
+                leg = mixed_vs_fp64(pkg, **kw)
                 pr = leg.pop("_prof")
                 leg["roofline_mixed"] = attempt_roofline(pr["mixed"], kw["n"], True, hbm,
                                                          fp64_tf, tf32_tf)

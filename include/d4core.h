@@ -208,6 +208,14 @@ int d4_solve(void *ctx, const double *g, double *dx);
 
 /* Reset the per-dislocation tolerances (PrecisionHandler::reset). */
 int d4_reset_tolerance(void *ctx);
+/* The per-dislocation tolerances (length n).  With d4_get_positions and the
+ * run result's sim_time and step_size they are the whole state the stepping
+ * loop carries from one accepted step to the next, so d4_set_positions,
+ * d4_set_time and d4_set_tolerance restart a context exactly where another
+ * (or a saved copy) stood.  The tolerances are squared distances;
+ * d4_set_tolerance rejects negative or non-finite values with D4_ERR_ARG. */
+int d4_get_tolerance(void *ctx, double *tol);
+int d4_set_tolerance(void *ctx, const double *tol);
 
 /* One attempted step from the context's positions at t0 with step h. The
  * big-step and two half-step positions stay on the device (d4_get_attempt). */

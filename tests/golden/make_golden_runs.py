@@ -6,8 +6,8 @@ Run here (where the reference tree and oracle/_ref are present):
 Every array is an output of the reference core built from its own sources
 (oracle/_ref/libd4ref_exact.so: src/*.cpp of danieltuzes/2D4 compiled
 unmodified, -O2 -ffp-contract=off, with the project's UMFPACK shim):
-  c2_*   the headline workload's own step sequence: 200 accepted steps
-         (-C 199) at constant stress 0.05 (FixedRateProtocol(0.05, 0)),
+  c2_*   the headline workload's own step sequence: 100 accepted steps
+         (-C 99) at constant stress 0.05 (FixedRateProtocol(0.05, 0)),
          default precision, from the relaxed N=1024 state of
          c2_relaxed_1024.npz; final positions and the accepted/failed counts;
   c3_*   N=4096 (seed 1002, iid uniform, balanced signs), dense Jacobian, 20
@@ -79,7 +79,7 @@ def case(name):
         path = os.path.join(tmp, "c2.dconf")
         write_dconf(dconf, path, z["x"], z["y"])
         ref = pyoracle.Reference("exact")
-        p = ref.params(step_count_limit=199, const_external_stress=0.05, has_rate=1, rate=0.0)
+        p = ref.params(step_count_limit=99, const_external_stress=0.05, has_rate=1, rate=0.0)
         xr, yr, res, wall = ref.run(path, p)
     elif name == "c3":
         import scipy
