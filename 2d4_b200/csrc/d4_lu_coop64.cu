@@ -10,10 +10,9 @@
 //
 // Schedule.  The matrix is processed in 32-column blocks by all CTAs of a
 // cooperative launch, separated by a grid barrier:
-//   pass   the first warp of every CTA eliminates the 32x32 diagonal block
-//          (redundantly, lane r holding row r in registers), then the CTAs
-//          eliminate the block's 32 columns for the rows below it (one thread
-//          per row, the row in registers), WITHOUT pivoting, starting from a
+//   pass   every CTA eliminates the block's 32 columns for its rows below the
+//          diagonal block, and all CTAs redundantly eliminate the 32x32
+//          diagonal block in shared memory, WITHOUT pivoting, starting from a
 //          saved copy P0 of the block's columns with the swaps found so far
 //          applied.  Pre-division values go to Q; a 32-bit mask records the
 //          columns where partial pivoting would have swapped (some
@@ -24,8 +23,8 @@
 //          appended to the block's list and the pass repeats.  A row swap at
 //          column k commutes with the updates of earlier columns, so applying
 //          the list to P0 up front is exact.
-//   finish CTAs apply the block's swaps to the other columns and solve
-//          U12 = L11^-1 A12 (one thread per column, the column in registers).
+//   finish CTAs write their rows' multipliers, apply the block's swaps to the
+//          other columns and solve U12 = L11^-1 A12 (warp per column).
 //   update trailing A22 -= L21 U12 in 64x64 tiles, the next tile's operands
 //          loaded while the current one computes; tiles that hold the next
 //          block's columns also refresh P0.  The oracle skips an update whose

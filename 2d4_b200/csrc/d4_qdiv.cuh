@@ -60,23 +60,5 @@ __device__ __forceinline__ float div(float a, float b, float y) {
     return a / b;
 }
 
-// The same quotient for a whole warp without divergent branches: the window
-// path for every lane, a select for zero numerators, and the division only
-// when some lane of the warp is outside the window (rare; all lanes of the
-// warp must call this together).
-template <typename T>
-__device__ __forceinline__ T div_warp(T a, T b, T y) {
-    const T q0 = a * y;
-    const T q1 = fma(fma(-b, q0, a), y, q0);
-    T q = fma(fma(-b, q1, a), y, q1);
-    const bool zero = a == T(0);
-    const bool ok = y != T(0) && (zero || in_range(a));
-    q = zero ? q0 : q;
-    if (__any_sync(0xffffffffu, !ok)) {
-        if (!ok) q = a / b;
-    }
-    return q;
-}
-
 }  // namespace qdiv
 }  // namespace d4
