@@ -94,7 +94,7 @@ SIGNATURES = {
     "d4_wait_selftest": (C.c_int, [_vp, C.c_int]),
     "d4_solver_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 4),
     "d4_lu_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 3),
-    "d4_mixed_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 3 + [_dp]),
+    "d4_mixed_stats": (C.c_int, [_vp] + [C.POINTER(C.c_longlong)] * 4 + [_dp]),
     "d4_set_block_lu": (C.c_int, [_vp, C.c_int]),
     "d4_pair_tile_threads": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "d4_ensemble_pair_tile_threads": (C.c_int, [_vp, C.POINTER(C.c_int)]),

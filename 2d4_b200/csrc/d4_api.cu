@@ -191,9 +191,21 @@ void read_async_errors(Ctx &c) {
     check_async_errors(c);
 }
 
-// Mixed form: attempts run on the FP64 path after a fallback before the block
-// LU is tried again.
-constexpr int kSkipAfterFallback = 16;
+// Mixed form backoff: after the f-th attempt in a row that neither the block
+// LU nor the pivoted FP32 LU could refine, the next 2^(f-1) attempts (at most
+// kMaxSkip) run on the FP64 path; after the b-th block-LU failure in a row the
+// next 2^(b-1) - 1 attempts use the pivoted FP32 LU directly.  A successful
+// block-LU attempt resets b, an attempt that FP32 factors refine resets f, so
+// a stretch of states that defeats a path wastes at most one try of it in
+// kMaxSkip attempts.
+constexpr int kMaxSkip = 64;
+
+// Below this order the mixed form's attempts run on the FP64 path: there the
+// exact LU is bound by its per-block latency, not by its arithmetic, so FP32
+// factors save little, while their refinement (and, for the stiff Jacobians of
+// close pairs, the fallbacks) costs more than the FP64 solves (measured at
+// N = 1024 over 300 steps of the relaxed state: 0.6x the FP64 form).
+constexpr int kMixedMinN = 2048;
 
 // Grid split of an attempt's two concurrent cooperative factorisations:
 // stage I's chain (one LU, two solves, one sweep) is the shorter one, so it
@@ -348,7 +360,11 @@ static double worst_refined(const unsigned long long *rb) {
         std::memcpy(&r, &rb[2 * k], 8);
         std::memcpy(&g, &rb[2 * k + 1], 8);
         if (std::isnan(r) || std::isnan(g)) return NAN;  // a NaN must fail the checks
-        if (g > 0) worst = std::max(worst, r / g);
+        if (g > 0) {
+            const double q = r / g;
+            if (!std::isfinite(q)) return NAN;  // inf / inf as well
+            worst = std::max(worst, q);
+        }
     }
     return worst;
 }
@@ -597,36 +613,80 @@ static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res, boo
 }
 
 // One attempted step.  In the mixed form the factorisations are block LUs
-// without row interchanges (d4_blu32.cu); when one of them met a zero or
-// non-finite pivot in a diagonal tile, or a refined solve kept a residual
-// above kRefineLimit, the attempt is redone with the pivoted cooperative LU,
-// so its result is that of the exact-pivoting path.
+// without row interchanges between tiles (d4_blu32.cu); when one of them met
+// a zero or non-finite pivot in a diagonal tile, or a refined solve kept a
+// residual above kRefineLimit, the attempt is redone with the pivoted FP32 LU
+// and, if its refinement fails too, with the FP64 form's attempt, so an
+// accepted result always carries a refined residual within kRefineLimit or
+// the FP64 form's solves.
 int attempt(Ctx &c, double t0, double h, d4_attempt_result *res) {
     if (c.p.precision != D4_PREC_MIXED) return attempt_once(c, t0, h, res);
-    if (!c.m_fast || c.m_skip > 0) {
-        // the FP64 form's attempt: block LU switched off, or a recent fallback
-        if (c.m_skip > 0) --c.m_skip;
+    auto fp32_ok = [&]() {
+        return !res->singular && res->refine_residual <= d4::kRefineLimit &&
+               std::isfinite(res->ratio);
+    };
+    auto fp64_attempt = [&]() {
         ++c.m_fp64_attempts;
         attempt_once(c, t0, h, res, true);
+        d4::adopt_pivots(c);  // the next block LUs factorise P A with this attempt's P
+    };
+    auto pivoted_attempt = [&]() {
+        ++c.m_pivoted32;
+        c.m_fast = 0;
+        try {
+            attempt_once(c, t0, h, res);
+        } catch (...) {
+            c.m_fast = 1;
+            throw;
+        }
+        c.m_fast = 1;
         d4::adopt_pivots(c);
+    };
+    if (!c.m_fast || c.m_skip > 0 || c.n < kMixedMinN) {
+        // the FP64 form's attempt: block LU switched off, a recent attempt
+        // that FP32 factors could not refine, or a system too small to gain
+        if (c.m_skip > 0) --c.m_skip;
+        fp64_attempt();
         return D4_OK;
     }
-    const long long before = c.m_blocklu;
-    attempt_once(c, t0, h, res);
-    if (c.m_blocklu == before) return D4_OK;  // no dense factorisation ran (GMRES)
-    const double rr = res->refine_residual;
-    if (!res->singular && rr <= d4::kRefineLimit) {
-        if (rr > c.m_worst_refine) c.m_worst_refine = rr;
-        return D4_OK;
+    if (c.m_piv_skip > 0) {
+        // a recent block-LU failure: the pivoted FP32 LU directly
+        --c.m_piv_skip;
+        pivoted_attempt();
+        if (fp32_ok()) {
+            if (res->refine_residual > c.m_worst_refine) c.m_worst_refine = res->refine_residual;
+            return D4_OK;
+        }
+    } else {
+        const long long before = c.m_blocklu;
+        attempt_once(c, t0, h, res);
+        if (c.m_blocklu == before) return D4_OK;  // no dense factorisation ran (GMRES)
+        if (fp32_ok()) {
+            if (res->refine_residual > c.m_worst_refine) c.m_worst_refine = res->refine_residual;
+            c.m_block_run = 0;
+            c.m_fallback_run = 0;
+            return D4_OK;
+        }
+        // a diagonal tile met a bad pivot or the refinement did not converge:
+        // the explicit inverses of the diagonal tiles lose accuracy when a tile
+        // is ill-conditioned (close pairs), which the backward-stable pivoted
+        // FP32 LU does not; it redoes the attempt, and the next block LUs wait
+        // 2^(b-1) attempts after the b-th failure in a row (at most kMaxSkip)
+        ++c.m_fallbacks;
+        c.m_piv_skip = std::min(kMaxSkip, 1 << std::min(c.m_block_run, 6)) - 1;
+        ++c.m_block_run;
+        pivoted_attempt();
+        if (fp32_ok()) {
+            if (res->refine_residual > c.m_worst_refine) c.m_worst_refine = res->refine_residual;
+            c.m_fallback_run = 0;
+            return D4_OK;
+        }
     }
-    // the refinement did not converge (the Jacobian too ill-conditioned for FP32
-    // factors) or a diagonal tile met a bad pivot: the FP64 form's attempt, and
-    // the next kSkipAfterFallback attempts go there directly
-    ++c.m_fallbacks;
-    ++c.m_fp64_attempts;
-    c.m_skip = kSkipAfterFallback;
-    attempt_once(c, t0, h, res, true);
-    d4::adopt_pivots(c);  // the next block LUs factorise P A with this attempt's P
+    // the Jacobian is too ill-conditioned for FP32 factors: the FP64 form's
+    // attempt, and the next attempts go there directly (backing off, kMaxSkip)
+    c.m_skip = std::min(kMaxSkip, 1 << std::min(c.m_fallback_run, 6));
+    ++c.m_fallback_run;
+    fp64_attempt();
     return D4_OK;
 }
 
@@ -1364,12 +1424,14 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
 }
 
 int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
-                   long long *fp64_attempts, double *worst_refined) {
+                   long long *pivoted_attempts, long long *fp64_attempts, double *worst_refined) {
     Ctx *c = (Ctx *)ctx;
-    if (!c || !block_factorizations || !fallbacks || !fp64_attempts || !worst_refined)
+    if (!c || !block_factorizations || !fallbacks || !pivoted_attempts || !fp64_attempts ||
+        !worst_refined)
         return D4_ERR_ARG;
     *block_factorizations = c->m_blocklu;
     *fallbacks = c->m_fallbacks;
+    *pivoted_attempts = c->m_pivoted32;
     *fp64_attempts = c->m_fp64_attempts;
     *worst_refined = c->m_worst_refine;
     return D4_OK;

@@ -57,7 +57,7 @@ constexpr size_t kRingBytes = (size_t)kStages * kStageBytes;
 constexpr size_t kBarOff = kRingBytes;   // barriers: full[3], empty[3], acc
 constexpr size_t kSmemBytes = kRingBytes + 1024;
 constexpr long long kSpin = 1ll << 24;   // flag polls (each >= 64 ns): > 1 s
-static_assert((size_t)kB * kSp * 4 + 4096 <= kRingBytes, "plain tile and GJ buffers fit the ring");
+static_assert((size_t)kB * kSp * 4 + 8 * kB * 4 <= kRingBytes, "plain tile and GJ buffers fit the ring");
 
 struct Args {
     int n, T;
@@ -136,22 +136,26 @@ __device__ __forceinline__ void ld64(uint32_t taddr, float (&v)[64]) {
 }
 
 // A tile F (plain, row-major, stride kSp, in shared memory) of tile position
-// (ti, tj) to LU (real entries) and to its operand slot: A format (rows as M)
-// when !bfmt, else B format (columns as N).
+// (ti, tj): store_tile writes its operand slot (A format, rows as M, when
+// !bfmt, else B format, columns as N), store_plain its real entries to LU.
+// The slot is what other tiles wait for; LU is read only by the solves, after
+// the launch, so it is written after the tile's flag is published.
+__device__ void store_plain(const Args &a, const float *Sp, int ti, int tj) {
+    const int tid = threadIdx.x;
+    const int n = a.n;
+    const int r = tid & 127, h = tid >> 7;
+    const int gr = ti * kB + r;
+    if (gr < n) {
+        for (int c = 64 * h; c < 64 * h + 64; ++c) {
+            const int gc = tj * kB + c;
+            if (gc < n) a.LU[(size_t)gr + (size_t)gc * n] = Sp[r * kSp + c];
+        }
+    }
+}
+
 __device__ void store_tile(const Args &a, const float *Sp, int ti, int tj, bool bfmt,
                            unsigned char *slot) {
     const int tid = threadIdx.x;
-    const int n = a.n;
-    {
-        const int r = tid & 127, h = tid >> 7;
-        const int gr = ti * kB + r;
-        if (gr < n) {
-            for (int c = 64 * h; c < 64 * h + 64; ++c) {
-                const int gc = tj * kB + c;
-                if (gc < n) a.LU[(size_t)gr + (size_t)gc * n] = Sp[r * kSp + c];
-            }
-        }
-    }
 #pragma unroll 4
     for (int u = 0; u < 16; ++u) {
         const int p = tid + kThreads * u;
@@ -172,12 +176,15 @@ __device__ void store_tile(const Args &a, const float *Sp, int ti, int tj, bool 
 
 // In-place Gauss-Jordan inverse of the 128 x 128 tile in Sp (no pivoting):
 // thread (tr, tc) of a 16 x 16 grid keeps rows 8tr.. and columns 8tc.. in
-// registers; per pivot k the owners of column k and row k publish them to
-// shared memory (double-buffered), one barrier, then every thread applies
+// registers.  The step of pivot k is the rank-1 form
 //     a_rc <- [c != k] a_rc - L_r U_c  (+1 at r = c = k)
-// with L_r = a_rk (a_kk - 1 at r = k) and U_c = a_kc / a_kk (1 / a_kk at c = k),
-// which is the in-place Gauss-Jordan step.  Returns false (on thread 0) when a
-// pivot is zero or not finite.
+// with L_r = a_rk (a_kk - 1 at r = k) and U_c = a_kc / a_kk (1 / a_kk at
+// c = k).  Pivots go in pairs (k, k+1) with one block barrier per pair: the
+// owners publish columns k, k+1 and rows k, k+1 as they stand before pivot k
+// (double-buffered), and every thread forms column k+1 and row k+1 after
+// pivot k for its own rows and columns with the same products the owners
+// would use, so the result is the one-pivot-at-a-time inverse bit for bit.
+// Returns false (on thread 0) when a pivot is zero or not finite.
 __device__ bool gauss_jordan(float *Sp, float *cbuf, float *rbuf) {
     const int tid = threadIdx.x;
     const int tr = tid >> 4, tc = tid & 15;
@@ -187,34 +194,52 @@ __device__ bool gauss_jordan(float *Sp, float *cbuf, float *rbuf) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) a[i][j] = Sp[(8 * tr + i) * kSp + 8 * tc + j];
     bool ok = true;
-    // pivots in groups of 8: the group index kb is a loop variable, the pivot's
+    // pivots in groups of 8: the group index kb is a loop variable, the pair's
     // place kl inside the group is a compile-time index into the registers
 #pragma unroll 1
     for (int kb = 0; kb < kB / 8; ++kb)
 #pragma unroll
-    for (int kl = 0; kl < 8; ++kl) {
+    for (int kl = 0; kl < 8; kl += 2) {
         const int k = 8 * kb + kl;
-        float *cb = cbuf + (kl & 1) * kB;
-        float *rb = rbuf + (kl & 1) * kB;
+        float *cb = cbuf + ((kl >> 1) & 1) * 2 * kB;  // columns k, k+1
+        float *rb = rbuf + ((kl >> 1) & 1) * 2 * kB;  // rows k, k+1
         if (tc == kb) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) cb[8 * tr + i] = a[i][kl];
+            for (int i = 0; i < 8; ++i) {
+                cb[8 * tr + i] = a[i][kl];
+                cb[kB + 8 * tr + i] = a[i][kl + 1];
+            }
         }
         if (tr == kb) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) rb[8 * tc + j] = a[kl][j];
+            for (int j = 0; j < 8; ++j) {
+                rb[8 * tc + j] = a[kl][j];
+                rb[kB + 8 * tc + j] = a[kl + 1][j];
+            }
         }
         __syncthreads();
+        // ---- pivot k
         const float akk = rb[k];
         const float p = 1.0f / akk;
         if (tid == 0 && !(isfinite(p) && akk != 0.f)) ok = false;
-        float L[8], U[8];
+        float L[8], U[8], C1[8], R1[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) L[i] = cb[8 * tr + i];
 #pragma unroll
         for (int j = 0; j < 8; ++j) U[j] = rb[8 * tc + j] * p;
         if (tc == kb) U[kl] = p;
         if (tr == kb) L[kl] = akk - 1.f;
+        // column k+1 (own rows) and row k+1 (own columns) after pivot k
+        const float uk1 = rb[k + 1] * p;  // U at column k+1
+        const float lk1 = rb[kB + k];     // L at row k+1: a_{k+1,k}
+#pragma unroll
+        for (int i = 0; i < 8; ++i) C1[i] = fmaf(-L[i], uk1, cb[kB + 8 * tr + i]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float r0 = rb[kB + 8 * tc + j];
+            R1[j] = (tc == kb && j == kl) ? -lk1 * U[j] : fmaf(-lk1, U[j], r0);
+        }
+        const float ak1 = fmaf(-lk1, uk1, rb[kB + k + 1]);  // a_{k+1,k+1} after pivot k
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
 #pragma unroll
@@ -226,6 +251,26 @@ __device__ bool gauss_jordan(float *Sp, float *cbuf, float *rbuf) {
             }
         }
         if (tr == kb && tc == kb) a[kl][kl] += 1.f;
+        // ---- pivot k+1
+        const float p2 = 1.0f / ak1;
+        if (tid == 0 && !(isfinite(p2) && ak1 != 0.f)) ok = false;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) U[j] = R1[j] * p2;
+        if (tc == kb) U[kl + 1] = p2;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) L[i] = C1[i];
+        if (tr == kb) L[kl + 1] = ak1 - 1.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (j == kl + 1)
+                    a[i][j] = (tc == kb) ? -L[i] * U[j] : fmaf(-L[i], U[j], a[i][j]);
+                else
+                    a[i][j] = fmaf(-L[i], U[j], a[i][j]);
+            }
+        }
+        if (tr == kb && tc == kb) a[kl + 1][kl + 1] += 1.f;
     }
     __syncthreads();
 #pragma unroll
@@ -267,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
     int *task_s = reinterpret_cast<int *>(sm + kBarOff + 192);
     float *Sp = reinterpret_cast<float *>(sm);
     float *cbuf = Sp + kB * kSp;
-    float *rbuf = cbuf + 2 * kB;
+    float *rbuf = cbuf + 4 * kB;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int n = a.n, T = a.T;
     const uint32_t ring = bulk::smem_u32(sm);
@@ -449,11 +494,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
             __syncthreads();
             store_tile(a, Sp, i, j, false, slot);
         }
-        // publish the tile
+        // publish the tile, then its plain entries (Sp stays intact until the
+        // next task's barrier)
         fence_async_global();
         __threadfence();
         __syncthreads();
         if (tid == 0) st_rel(&a.ready[i * T + j], a.epoch);
+        store_plain(a, Sp, i, j);
     }
     coop::tc::fence_before();
     __syncthreads();

@@ -171,7 +171,11 @@ struct Ctx {
     BluState blu_state, blu_state_b;
     int m_blk = 0, m_blk_b = 0;  // Mix32Bufs::blk of the primary and stage-I buffer sets
     long long m_blocklu = 0, m_fallbacks = 0, m_fp64_attempts = 0;
-    int m_skip = 0;  // attempts left on the FP64 path after a fallback
+    int m_skip = 0;          // attempts left on the FP64 path (backoff)
+    int m_fallback_run = 0;  // attempts in a row that no FP32 factorisation refined
+    int m_piv_skip = 0;      // attempts left on the pivoted FP32 LU (backoff)
+    int m_block_run = 0;     // block-LU failures in a row
+    long long m_pivoted32 = 0;  // attempts run with the pivoted FP32 LU
     double m_worst_refine = 0;
 
     // cutoff sparse path: CSR of the matrix and the GMRES work space

@@ -15,8 +15,9 @@ constexpr int kThreads = 256;
 constexpr long long kSpinLimit = 1ll << 24;  // x >= 64 ns each: > 1 s
 constexpr int kGenWord = 32;
 // Dynamic shared memory: the narrow last block's rows (a row of NB + 1 entries
-// per thread, also the trailing update's second piece buffer), the diagonal
-// block's pre-division values (NB rows), and for the FP32 form after them the four
+// per thread) and the diagonal block's pre-division values (NB rows) during a
+// pass, the trailing update's second piece buffer during the update; for the
+// FP32 form after them the four
 // tensor-core operand tiles (L21 and U12 as TF32 hi and lo parts, 16 KiB each,
 // 1 KiB aligned) plus the MMA completion barrier and the TMEM address slot.
 constexpr size_t kOpTileBytes = 128 * NB * 4;

@@ -364,13 +364,15 @@ class Engine:
         return dict(zip(("factorizations", "passes", "swaps"), [t.value for t in v]))
 
     def mixed_stats(self):
-        """Mixed form's factorisations (d4_mixed_stats): block LUs run, attempts
-        redone on the FP64 path, attempts on the FP64 path in all, worst refined
-        residual of the block-LU attempts that stood."""
-        b, f, a, w = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_double()
-        self._call("d4_mixed_stats", C.byref(b), C.byref(f), C.byref(a), C.byref(w))
+        """Mixed form's factorisations (d4_mixed_stats): block LUs run, block-LU
+        attempts that failed, attempts run with the pivoted FP32 LU, attempts on
+        the FP64 path, worst refined residual of the FP32 attempts that stood."""
+        b, f, p, a, w = (C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_longlong(),
+                         C.c_double())
+        self._call("d4_mixed_stats", C.byref(b), C.byref(f), C.byref(p), C.byref(a), C.byref(w))
         return {"block_factorizations": b.value, "fallbacks": f.value,
-                "fp64_attempts": a.value, "worst_refined_residual": w.value}
+                "pivoted_fp32_attempts": p.value, "fp64_attempts": a.value,
+                "worst_refined_residual": w.value}
 
     def set_block_lu(self, enable=True):
         """Mixed form: block LU with per-attempt fallback (default), or every

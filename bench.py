@@ -71,6 +71,9 @@ WORKLOADS = {
                desc="N=64 plain FP64, tau_ext=0, P=1e-8"),
     "c3-fp64": dict(n=4096, tau=0.1, precision=1e-5, source=("seed", 1002),
                     desc="N=4096 plain FP64, dense Jacobian, tau_ext=0.1"),
+    "c3-mixed": dict(n=4096, tau=0.1, precision=1e-5, source=("seed", 1002), mixed=True,
+                     desc="N=4096 mixed form (FP64 sweeps and residuals, FP32 block LU on the "
+                          "tensor cores, refined solves), dense Jacobian, tau_ext=0.1"),
     "c4": dict(n=None, tau=0.0, precision=1e-5, source="ensemble",
                desc="512-instance ensemble, N_k uniform over even values in [64, 2048], "
                     "tau_ext = 1e-3 t, sharded over the ranks (one ensemble per GPU)"),
@@ -179,6 +182,8 @@ def make_sd(pkg, x, y, wl):
     sd.set_positions(x, y)
     sd.precision = wl["precision"]
     sd.external_stress = pkg.FixedRateProtocol(wl["tau"], 0.0)
+    if wl.get("mixed"):
+        sd.precision_mode = pkg._lib.D4_PREC_MIXED
     return sd
 
 
@@ -418,7 +423,8 @@ def mixed_vs_fp64(pkg, n, seed, tau, steps, start=None, free_steps=200, report_e
             "free_run_diff_vs_fp64": {"columns": ["step", "mixed", "fp64 from x0 + 1e-15"],
                                       "rows": curve},
             "mixed_block_factorizations": ms["block_factorizations"],
-            "mixed_fallbacks_to_fp64": ms["fallbacks"],
+            "mixed_block_lu_fallbacks": ms["fallbacks"],
+            "mixed_pivoted_fp32_attempts": ms["pivoted_fp32_attempts"],
             "mixed_fp64_path_attempts": ms["fp64_attempts"],
             "mixed_worst_refined_residual": ms["worst_refined_residual"],
             "fp64_ms_per_call": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof["fp64"].items()},
@@ -746,13 +752,16 @@ def main():
         return
     hbm, bf16, peak_src = measured_peaks()
     fp64_tf = fp64_peak_tflops(torch, device)
-    roof = roofline(prof, n, hbm, fp64_tf)
+    roof = attempt_roofline(prof, n, bool(wl.get("mixed")), hbm, fp64_tf, bf16 / 2)
     roof["hbm_peak_source"] = peak_src
     line = {"metric": "dislocation-steps/s", "value": value, "unit": "dislocation-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl["desc"], "n": n, "form": "plain FP64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (linear algebra tf32x3 refined in f64)" if wl.get("mixed") else "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["desc"], "n": n,
+                       "form": "mixed" if wl.get("mixed") else "plain FP64",
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "flushed between steps (512 MiB write)",
                        "timed_steps": "accepted steps 1..K from the workload's start (warm-up "

@@ -257,14 +257,17 @@ int d4_lu_stats(void *ctx, long long *factorizations, long long *passes, long lo
 
 /* Mixed form's factorisations (no counterpart in the reference): block LU
  * factorisations run (128 x 128 tiles on the tensor cores, no row interchanges
- * between tiles, rows in the order of the last FP64 factorisation), attempts
- * redone on the FP64 form's path because a diagonal tile met a zero or
- * non-finite pivot or the refinement left max|g - A dx| above 1e-9 max|g| (the
- * Jacobian too ill-conditioned for FP32 factors), attempts that ran on the FP64
- * path in all (the redone ones and the 16 after each), and the worst refined
- * residual of the block-LU attempts that stood. */
+ * between tiles, rows in the order of the last pivoted factorisation);
+ * fallbacks: block-LU attempts in which a diagonal tile met a zero or
+ * non-finite pivot or the refinement left max|g - A dx| above 1e-9 max|g|;
+ * attempts run with the pivoted FP32 LU (each fallback redone, and the
+ * attempts after the b-th fallback in a row, 2^(b-1) - 1 of them, at most
+ * 63; the next block LUs use its row order); attempts that ran on the FP64
+ * form's path (an attempt that the pivoted FP32 LU could not refine either,
+ * and the attempts after the f-th such in a row, 2^(f-1) of them, at most
+ * 64); and the worst refined residual of the FP32 attempts that stood. */
 int d4_mixed_stats(void *ctx, long long *block_factorizations, long long *fallbacks,
-                   long long *fp64_attempts, double *worst_refined);
+                   long long *pivoted_attempts, long long *fp64_attempts, double *worst_refined);
 
 /* Mixed form: enable = 1 (the default) runs attempts on the block LU with the
  * fallback that d4_mixed_stats describes; 0 runs every attempt on the FP64
@@ -278,12 +281,6 @@ int d4_set_block_lu(void *ctx, int enable);
  * the process; the results do not depend on the choice).  threads_y = 0 until
  * then. */
 int d4_pair_tile_threads(void *ctx, int *threads_y);
-
-/* Mixed form: enable = 1 (the default) factorises with the block LU and
- * falls back per attempt as d4_mixed_stats describes; 0 always uses the
- * pivoted cooperative LU (exact partial pivoting, as the FP64 form).  No
- * counterpart in the reference. */
-int d4_set_block_lu(void *ctx, int enable);
 
 /* Batched ensemble of independent systems: the many-realisation statistics
  * workload, where the reference runs one system per process

@@ -31,9 +31,10 @@ def run(pkg, mode, overlap, n, seed, steps):
     return r, xe, st
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed"])
-@pytest.mark.parametrize("n,seed", [(256, 11), (600, 12)])
+@pytest.mark.parametrize("form,n,seed", [("fp64", 256, 11), ("fp64", 600, 12),
+                                         ("mixed", 2048, 12)])
 def test_overlap_matches_sequential(pkg, form, n, seed):
+    """(The mixed form's FP32 factorisations run from N = 2048 on.)"""
     mode = pkg._lib.D4_PREC_MIXED if form == "mixed" else pkg._lib.D4_PREC_FP64
     ra, xa, sa = run(pkg, mode, True, n, seed, 12)
     rb, xb, sb = run(pkg, mode, False, n, seed, 12)
@@ -42,7 +43,8 @@ def test_overlap_matches_sequential(pkg, form, n, seed):
     assert ra.strain == rb.strain
     assert np.array_equal(xa, xb)
     assert sa == sb
-    assert sa["factorizations"] == 3 * ra.attempts
+    if form == "fp64":
+        assert sa["factorizations"] == 3 * ra.attempts
 
 
 @pytest.mark.parametrize("form", ["fp64", "mixed"])
@@ -50,7 +52,7 @@ def test_overlap_single_attempt(pkg, form):
     """One attempt from the same state: every stage's positions, the error
     ratio and the refined residual agree bit for bit."""
     mode = pkg._lib.D4_PREC_MIXED if form == "mixed" else pkg._lib.D4_PREC_FP64
-    x, y, _ = pkg.dconf.generate_internal(512, 1002)
+    x, y, _ = pkg.dconf.generate_internal(2048 if form == "mixed" else 512, 1002)
     out = []
     for overlap in (True, False):
         sd = pkg.SimulationData()
@@ -59,7 +61,7 @@ def test_overlap_single_attempt(pkg, form):
         sd.external_stress = pkg.FixedRateProtocol(0.1, 0.0)
         e = pkg.Engine(sd)
         e.set_overlap(overlap)
-        out.append(e.attempt(0.0, 3e-7))
+        out.append(e.attempt(0.0, 1e-7))
         e.close()
     (ra, *xa), (rb, *xb) = out
     for a, b in zip(xa, xb):
