@@ -641,7 +641,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed vs FP64 legs")
     ap.add_argument("--mixed-steps", type=int, default=0,
                     help="shadowed accepted steps of the mixed vs FP64 legs (default: 200 at "
-                         "N=4096, 1000 at N=1024)")
+                         "N=4096, 300 at N=1024, where the mixed form runs the FP64 path)")
     ap.add_argument("--legs", default="cutoff,tabulated,ensemble,adjoint,xpattern",
                     help="extra single-GPU legs (comma list, or 'none')")
     args = ap.parse_args()
@@ -782,7 +782,7 @@ def main():
         tf32_tf = bf16 / 2
         for key, kw in (("mixed_vs_fp64", dict(n=4096, seed=1002, tau=0.1, steps=200,
                                                free_steps=100, report_every=10)),
-                        ("mixed_vs_fp64_n1024", dict(n=1024, seed=1001, tau=0.05, steps=1000,
+                        ("mixed_vs_fp64_n1024", dict(n=1024, seed=1001, tau=0.05, steps=300,
                                                      start=start_state(pkg, WORKLOADS["c2"])))):
             try:
                 if args.mixed_steps > 0:
