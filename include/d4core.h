@@ -202,7 +202,7 @@ int d4_factor(void *ctx);
  * D4_WARN_SINGULAR like umfpack_di_solve and, like it, leaves the result as
  * computed; d4_attempt/d4_run apply solveEQSys's zeroing of entries outside
  * (-1, 1) (src/simulation.cpp:646-658) themselves.  Mixed form: the FP32
- * factors' solves refined in FP64 against the FP64 matrix (at most 4 sweeps,
+ * factors' solves refined in FP64 against the FP64 matrix (at most 6 sweeps,
  * stopping at max|g - A dx| <= 1e-12 max|g|). */
 int d4_solve(void *ctx, const double *g, double *dx);
 
