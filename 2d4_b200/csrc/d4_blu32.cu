@@ -863,6 +863,9 @@ void blu_alloc(BluBufs &B, int n, const int *tasks, BluState *state) {
     D4_CUDA_OK(d4::dmalloc((void **)&B.fx, sizeof(int) * (size_t)T));
     D4_CUDA_OK(d4::dmalloc((void **)&B.y, sizeof(float) * (size_t)T * blu::kB));
     D4_CUDA_OK(d4::dmalloc((void **)&B.xs, sizeof(float) * (size_t)T * blu::kB));
+    // ticket[0]: the factorisation's (zeroed before each launch); ticket[1]: the
+    // solves' (zero here, then reset by the CTA that takes a launch's last one)
+    D4_CUDA_OK(cudaMemset(B.ticket, 0, sizeof(int) * 4));
     D4_CUDA_OK(cudaMemset(B.ready, 0, sizeof(int) * (size_t)T * T));
     D4_CUDA_OK(cudaMemset(B.fy, 0, sizeof(int) * (size_t)T));
     D4_CUDA_OK(cudaMemset(B.fx, 0, sizeof(int) * (size_t)T));
