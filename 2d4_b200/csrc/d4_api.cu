@@ -499,12 +499,14 @@ static void attempt_overlap_mixed(Ctx &c, double t0, double h, int *singular_out
 
 // Stages I-IV of src/simulation.cpp:90-161 on the device.
 // fp64: in the mixed form, run this attempt on the FP64 form's factorisations
-// and solves (sequentially: the second stream's buffers are the mixed form's).
+// and solves (with stage I overlapped when the context holds the FP64 form's
+// stage-I buffers, as below kMixedMinN; else in sequence).
 static int attempt_once(Ctx &c, double t0, double h, d4_attempt_result *res, bool fp64 = false) {
-    if (c.overlap && !(fp64 && c.p.precision == D4_PREC_MIXED)) {
+    const bool mixed_path = c.p.precision == D4_PREC_MIXED && !fp64;
+    if (c.overlap && (mixed_path || c.lub.LU)) {
         int singular = 0;
         double refine = 0;
-        if (c.p.precision == D4_PREC_MIXED)
+        if (mixed_path)
             attempt_overlap_mixed(c, t0, h, &singular, &refine);
         else
             attempt_overlap(c, t0, h, &singular);
@@ -885,7 +887,10 @@ int d4_create(void **out, int n, const d4_params *p) {
             double **bv[] = {&c->dvec_b, &c->speed_b, &c->speed2_b, &c->xw1_b, &c->xw2_b,
                              &c->dx_b};
             for (double **v : bv) dalloc(v, (size_t)n);
-            if (!mixed) {
+            dalloc(&c->F_b, nn);
+            if (!mixed || n < kMixedMinN) {
+                // the FP64 form's stage I (also the mixed form's attempts below
+                // kMixedMinN, which run on the FP64 path)
                 dalloc(&c->lub.LU, nn);
                 dalloc(&c->lub.P0, (size_t)n * 32);
                 dalloc(&c->lub.Q, (size_t)n * 64);
@@ -893,10 +898,9 @@ int d4_create(void **out, int n, const d4_params *p) {
                 dalloc(&c->lub.bar, 64);
                 dalloc(&c->lub.perm, (size_t)n);
                 dalloc(&c->lub.piv, (size_t)n);
-                dalloc(&c->F_b, nn);
-            } else {
+            }
+            if (mixed) {
                 d4::Mix32Bufs &B = c->m32b;
-                dalloc(&c->F_b, nn);
                 dalloc(&B.A64, nn);
                 dalloc(&B.conv, (size_t)d4::kIrMax + 1);
                 dalloc(&B.A32, nn);
