@@ -2,7 +2,7 @@
 """Throughput of the 2D4_sim implicit step on B200: dislocation-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c3-fp64] [--no-cpu-baseline] [--no-mixed]
+                    [--workload c2|c1|c3-fp64|c3-mixed|c4] [--no-cpu-baseline] [--no-mixed]
                     [--legs cutoff,tabulated,ensemble,adjoint,xpattern|none]
 
 A step is one ACCEPTED implicit step (stages I-IV of src/simulation.cpp:88-277;
@@ -32,13 +32,20 @@ N / that time.
 flags (oracle/_ref/libd4ref_fast.so, UMFPACK replaced by OpenBLAS dgetrf/dgetrs on
 all host cores) on the same workload, through Simulation::run, rank 0 only.
 
+Other workloads: c1 (N=64, tau = 0), c3-fp64 and c3-mixed (N=4096 dense,
+tau = 0.1, plain FP64 form or mixed form), c4 (the 512-instance ensemble
+sharded over the ranks of a torchrun job).
+
 At N=1 the line also carries bounded legs for the other configurations:
-mixed_vs_fp64 (N=4096 dense, tau = 0.1, and N=1024 from the relaxed start:
-the two forms in lockstep for --mixed-steps accepted steps, default 1000, with
-the position difference after every step), cutoff (N=4096, Heaviside c = 0.1: FP64 dense,
-FP64 GMRES, mixed GMRES), tabulated (the N=1024 workload with the tabulated
-field), ensemble (512 instances of uneven N), adjoint (N=2048, 200 steps) and
-xpattern (direct-Fourier pattern analysis, N=4096 at resolution 1024).
+mixed_vs_fp64 (N=4096 dense, tau = 0.1, 200 accepted steps, and N=1024 from
+the relaxed start, 300: the FP64 form takes each step and the mixed form
+restarts from its state and takes the same step, both timed, with the
+position difference after every step; then both forms and the FP64 form from
+positions moved by 1e-15 run free, their differences side by side), cutoff
+(N=4096, Heaviside c = 0.1: FP64 dense, FP64 GMRES, mixed GMRES), tabulated
+(the N=1024 workload with the tabulated field), ensemble (512 instances of
+uneven N), adjoint (N=2048, 200 steps, central differences on 32 coordinates)
+and xpattern (direct-Fourier pattern analysis, N=4096 at resolution 1024).
 """
 import argparse
 import glob
