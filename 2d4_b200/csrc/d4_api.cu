@@ -866,8 +866,8 @@ int d4_create(void **out, int n, const d4_params *p) {
         c->lu_grid = d4::coop_grid_size(n);
         if (c->lu_grid < 0) throw d4::StateError("n too large for the cooperative LU");
         dalloc(&c->lu_p0, (size_t)n * 32);
-        dalloc(&c->lu_q, (size_t)n * 64);
-        c->lu_mask_words = nblk * 33 + 8;
+        dalloc(&c->lu_q, (size_t)n * 64 + d4::kLuDiagWords);
+        c->lu_mask_words = d4::lu_mask_words_for(nblk);
         dalloc(&c->lu_mask, (size_t)c->lu_mask_words);
         dalloc(&c->lu_bar, 64);
         if (p->field == D4_FIELD_TABULATED) {
@@ -893,7 +893,7 @@ int d4_create(void **out, int n, const d4_params *p) {
                 // kMixedMinN, which run on the FP64 path)
                 dalloc(&c->lub.LU, nn);
                 dalloc(&c->lub.P0, (size_t)n * 32);
-                dalloc(&c->lub.Q, (size_t)n * 64);
+                dalloc(&c->lub.Q, (size_t)n * 64 + d4::kLuDiagWords);
                 dalloc(&c->lub.mask, (size_t)c->lu_mask_words);
                 dalloc(&c->lub.bar, 64);
                 dalloc(&c->lub.perm, (size_t)n);

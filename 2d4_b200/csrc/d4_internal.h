@@ -14,6 +14,13 @@ namespace d4 {
 
 constexpr int kTile = 32;          // pair tile edge
 constexpr int kLuNb = 32;          // LU block width (FP64 path)
+// Cooperative LU buffers: per launch one mask word per possible pass, then
+// the FP64 form's schedule words (tickets, strip counters, look-ahead epoch);
+// after the two Q halves (2 x n x 32) the published diagonal block and its
+// reciprocals.
+constexpr int lu_pass_words(int nblk) { return nblk * 33 + 8; }
+constexpr int lu_mask_words_for(int nblk) { return lu_pass_words(nblk) + nblk + 64; }
+constexpr int kLuDiagWords = kLuNb * (kLuNb + 1) + kLuNb + kLuNb * kLuNb;
 constexpr int kSolveThreads = 1024;
 constexpr int kMaxSolveN = 8192;   // x and g of the one-CTA solve live in shared memory
 

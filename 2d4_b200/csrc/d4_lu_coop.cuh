@@ -42,7 +42,19 @@ struct CoopArgs {
     int *piv;        // n pivot rows
     int *flags;      // kFlagSingular, kFlagBarrierTimeout, kFlagPasses, kFlagSwaps
     unsigned *bar;   // grid barrier: [0] arrivals, [kGenWord] generation
+    // FP64 form only (look-ahead of the next diagonal block during the
+    // trailing update), zeroed before the launch: per block kb the update's
+    // finished strip-0 tiles [kb]; [nblk] the last block whose diagonal block
+    // is published
+    unsigned *sched;
+    T *dg;           // kLuDiagWords: see kDiagWords (null in the FP32 form)
 };
+
+// dg: the published diagonal block s (NB x (NB + 1)), its reciprocals rs (NB),
+// then the next diagonal block's entries before the update (NB x NB, by column)
+constexpr int kDiagWords = NB * (NB + 1) + NB;
+constexpr int kSnapOffset = kDiagWords;
+static_assert(kDiagWords + NB * NB == kLuDiagWords && NB == kLuNb, "buffer sizes in d4_internal.h");
 
 __device__ __forceinline__ unsigned ld_acq(const unsigned *p) {
     unsigned v;
@@ -83,6 +95,27 @@ static __device__ void grid_barrier(unsigned *bar, int *flags, unsigned &gen, in
     __syncthreads();
 }
 
+__device__ __forceinline__ void st_rel(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Thread 0: wait until *p >= target, bounded as the grid barrier is (a CTA
+// that gives up records kFlagBarrierTimeout and stops waiting for good).
+__device__ __forceinline__ void wait_ge(const unsigned *p, unsigned target, int *flags,
+                                        int *dead_s) {
+    if (*dead_s) return;
+    long long spins = 0;
+    while (ld_acq(p) < target) {
+        __nanosleep(32);
+        if ((++spins & 255) == 0 &&
+            (spins > kSpinLimit || ld_acq((const unsigned *)&flags[kFlagBarrierTimeout]))) {
+            atomicOr(&flags[kFlagBarrierTimeout], 1);
+            *dead_s = 1;
+            return;
+        }
+    }
+}
+
 // Source row in P0 of position r after the block's transpositions (applied in
 // order to the arrangement): walk the list backwards.
 __device__ __forceinline__ int src_row(int r, const int *sa, const int *sb, int ns) {
@@ -105,16 +138,17 @@ template <typename T>
 __device__ __noinline__ unsigned diag_block(const CoopArgs<T> &a, T *Q, T (*s)[NB + 1],
                                             T *rs, T (*qbuf)[NB + 1], int k0, int kw,
                                             const int *sa, const int *sb, int ns, unsigned skip,
-                                            bool write_q) {
+                                            bool write_q, bool preloaded = false) {
     const int n = a.n;
     const int tid = threadIdx.x;
     unsigned msk = 0;
-    for (int t = tid; t < NB * NB; t += kThreads) {
-        const int r = t % NB, k = t / NB;
-        T v = 0.0;
-        if (r < kw && k < kw) v = a.P0[(size_t)src_row(k0 + r, sa, sb, ns) + (size_t)k * n];
-        s[r][k] = v;
-    }
+    if (!preloaded)
+        for (int t = tid; t < NB * NB; t += kThreads) {
+            const int r = t % NB, k = t / NB;
+            T v = 0.0;
+            if (r < kw && k < kw) v = a.P0[(size_t)src_row(k0 + r, sa, sb, ns) + (size_t)k * n];
+            s[r][k] = v;
+        }
     __syncthreads();
     for (int k = 0; k < kw; ++k) {
         const T d = s[k][k];
@@ -264,7 +298,8 @@ __device__ __noinline__ unsigned rows_below(const CoopArgs<T> &a, T *Q,
 // The block's row swaps on every other column, then U12 = L11^-1 A12 on the
 // columns right of the block, a warp per column: lane r holds row r, column
 // k's value reaches the lanes below by shuffle (u_kj == 0 skips its updates,
-// as the oracle does).
+// as the oracle does).  The FP64 form also keeps the next diagonal block's
+// entries (after the swaps, before the update) for the look-ahead.
 template <typename T>
 __device__ __noinline__ void finish_cols(const CoopArgs<T> &a, const T (*s)[NB + 1], int k0,
                                          int kw, const int *sa, const int *sb, int ns) {
@@ -283,6 +318,10 @@ __device__ __noinline__ void finish_cols(const CoopArgs<T> &a, const T (*s)[NB +
                 }
             }
             __syncwarp();
+            if (a.dg && j >= k0 + kw && j < k0 + kw + NB) {
+                const int nk0 = k0 + kw;
+                if (nk0 + lane < n) a.dg[kSnapOffset + (j - nk0) * NB + lane] = cj[nk0 + lane];
+            }
             if (j >= k0 + kw) {
                 T v = lane < kw ? cj[k0 + lane] : 0.0;
                 for (int k = 0; k < kw; ++k) {
@@ -307,21 +346,77 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Trailing update A22 -= L21 U12 of the plain form, every entry in the
 // oracle's order (k ascending, product and difference rounded separately);
-// tiles holding the next block's columns also refresh P0.  64 x 64 tiles,
-// 4 x 4 entries per thread.  While a tile computes, the next tile's L21 and
-// U12 pieces stream into the other shared-memory buffer (cp.async) and its
+// tiles holding the next block's columns (strip 0) also refresh P0.  64 x 64
+// tiles, 4 x 4 entries per thread.  While a tile computes, the next tile's L21
+// and U12 pieces stream into the other shared-memory buffer (cp.async) and its
 // entries into registers.
+//
+// Look-ahead: the last CTA takes no tile (unless it is the only one).  It
+// forms the next block's diagonal block itself from A, L21 and U12 (the same
+// operations in the same order as the tile that owns it, so the same values),
+// eliminates it as diag_block does for the next block's first pass (no swaps
+// yet) and publishes it: s and rs to dg, pre-division values to Q, flags into
+// the next pass's mask word.  The next pass starts without a grid barrier,
+// once the diagonal block is published and the strip-0 tiles (P0) are done.
 template <typename T>
-__device__ __noinline__ void update_tiles(const CoopArgs<T> &a, int k0, int kw, T *buf0,
-                                          T *buf1) {
+__device__ __noinline__ void update_la(const CoopArgs<T> &a, int k0, int kw, int kb, int pass,
+                                       T *buf0, T *buf1, T (*s)[NB + 1], T *rs,
+                                       T (*qbuf)[NB + 1], const int *sa, const int *sb,
+                                       unsigned *la_mask_s) {
     constexpr int kLd = 64 + 1;          // row stride of the L and U pieces
     constexpr int kPiece = NB * kLd;     // one piece (L or U)
     const int n = a.n, tid = threadIdx.x, cta = blockIdx.x, G = gridDim.x;
+    const int nblk = (n + NB - 1) / NB;
     const int base = k0 + kw, rest = n - base;
     const int tb = (rest + 63) / 64;
     const int nk0 = base, nkw = min(NB, n - base);  // next block's columns
     const int tr = tid % 16, tc = tid / 16;
     const int ntiles = tb * tb;
+    const int gt = G > 1 ? G - 1 : 1;  // CTAs that take tiles
+    if (cta == G - 1) {
+        // the next block's diagonal block: L and U pieces, then 4 entries per thread
+        T *Lp = buf0, *Up = buf0 + NB * (NB + 1);
+        for (int t = tid; t < NB * NB; t += kThreads) {
+            const int r = t % NB, k = t / NB;
+            Lp[k * (NB + 1) + r] = (r < nkw && k < kw) ? a.A[(size_t)(nk0 + r) + (size_t)(k0 + k) * n] : T(0);
+            const int k2 = t % NB, c = t / NB;
+            Up[k2 * (NB + 1) + c] = (c < nkw && k2 < kw) ? a.A[(size_t)(k0 + k2) + (size_t)(nk0 + c) * n] : T(0);
+        }
+        // the entries before the update come from the snapshot finish_cols
+        // took: the tile that owns them may already have overwritten A
+        T v[NB * NB / kThreads];
+#pragma unroll
+        for (int e = 0; e < NB * NB / kThreads; ++e) {
+            const int t = tid + e * kThreads, r = t % NB, c = t / NB;
+            v[e] = (r < nkw && c < nkw) ? __ldcg(a.dg + kSnapOffset + c * NB + r) : T(0);
+        }
+        __syncthreads();
+        for (int k = 0; k < kw; ++k) {
+#pragma unroll
+            for (int e = 0; e < NB * NB / kThreads; ++e) {
+                const int t = tid + e * kThreads, r = t % NB, c = t / NB;
+                v[e] = v[e] - Lp[k * (NB + 1) + r] * Up[k * (NB + 1) + c];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < NB * NB / kThreads; ++e) {
+            const int t = tid + e * kThreads;
+            s[t % NB][t / NB] = v[e];
+        }
+        if (tid == 0) *la_mask_s = 0;
+        T *Qn = a.Q + (size_t)(pass & 1) * n * NB;
+        const unsigned m = diag_block(a, Qn, s, rs, qbuf, nk0, nkw, sa, sb, 0, 0u, true, true);
+        if (m) atomicOr(la_mask_s, m);
+        for (int t = tid; t < kDiagWords; t += kThreads)
+            a.dg[t] = t < NB * (NB + 1) ? s[t / (NB + 1)][t % (NB + 1)] : rs[t - NB * (NB + 1)];
+        __syncthreads();
+        if (tid == 0) {
+            if (*la_mask_s) atomicOr(&a.mask[pass], *la_mask_s);
+            __threadfence();
+            st_rel(a.sched + nblk, (unsigned)(kb + 1));
+        }
+        if (G > 1) return;
+    }
     T pa[4][4];
     auto stage = [&](int tile, T *buf) {
         const int i0 = base + (tile % tb) * 64, j0 = base + (tile / tb) * 64;
@@ -347,7 +442,7 @@ __device__ __noinline__ void update_tiles(const CoopArgs<T> &a, int k0, int kw, 
     };
     if (cta < ntiles) stage(cta, buf0);
     int par = 0;
-    for (int tile = cta; tile < ntiles; tile += G, par ^= 1) {
+    for (int tile = cta; tile < ntiles; tile += gt, par ^= 1) {
         const int i0 = base + (tile % tb) * 64, j0 = base + (tile / tb) * 64;
         const T *Ls = par ? buf1 : buf0;
         const T *Us = Ls + kPiece;
@@ -358,7 +453,7 @@ __device__ __noinline__ void update_tiles(const CoopArgs<T> &a, int k0, int kw, 
             for (int q = 0; q < 4; ++q) acc[p][q] = pa[p][q];
         cp_async_wait_all();
         __syncthreads();  // this tile's pieces are in; the other buffer is free
-        if (tile + G < ntiles) stage(tile + G, par ? buf0 : buf1);
+        if (tile + gt < ntiles) stage(tile + gt, par ? buf0 : buf1);
 #pragma unroll 2
         for (int k = 0; k < kw; ++k) {
             T lv[4], uv[4];
@@ -382,7 +477,13 @@ __device__ __noinline__ void update_tiles(const CoopArgs<T> &a, int k0, int kw, 
                         a.P0[(size_t)gi + (size_t)(gj - nk0) * n] = acc[p][q];
                 }
             }
-        __syncthreads();  // the products are done with this buffer before it is refilled
+        // products done with this buffer before it is refilled; a strip-0
+        // tile's stores are in before it is counted
+        __syncthreads();
+        if (tile < tb && tid == 0) {
+            __threadfence();
+            atomicAdd(a.sched + kb, 1u);
+        }
     }
 }
 
@@ -492,6 +593,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
     __shared__ T red_v[kThreads / 32];
     __shared__ int red_i[kThreads / 32];
     __shared__ int dead_s;
+    __shared__ unsigned la_mask_s;        // look-ahead: flags of the diagonal block
 
     const int n = a.n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -539,6 +641,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
         }
         __syncthreads();
         int scan_from = 0;
+        bool first = true;
         // ------------------------------------------------------------ passes
         for (;;) {
             const int par = pass & 1;
@@ -546,10 +649,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
             const int ns = ns_s;
             const unsigned skip = skip_mask;
             if (tid == 0) cta_mask = 0;
-            // diagonal block, redundantly in every CTA, then the rows below
-            unsigned my_mask =
-                diag_block(a, Q, s, rs, reinterpret_cast<T (*)[NB + 1]>(rowbuf + kThreads * (NB + 1)),
-                           k0, kw, sa, sb, ns, skip, cta == 0);
+            unsigned my_mask = 0;
+            if (!kTc && kb > 0 && first) {
+                // the diagonal block published by the previous update's
+                // look-ahead, once that update's strip 0 (P0) is done too
+                if (tid == 0) {
+                    wait_ge(a.sched + nblk, (unsigned)kb, a.flags, &dead_s);
+                    wait_ge(a.sched + (kb - 1), (unsigned)((n - k0 + 63) / 64), a.flags, &dead_s);
+                }
+                __syncthreads();
+                for (int t = tid; t < kDiagWords; t += kThreads) {
+                    const T v = __ldcg(a.dg + t);
+                    if (t < NB * (NB + 1))
+                        s[t / (NB + 1)][t % (NB + 1)] = v;
+                    else
+                        rs[t - NB * (NB + 1)] = v;
+                }
+                __syncthreads();
+            } else {
+                // diagonal block, redundantly in every CTA
+                my_mask = diag_block(a, Q, s, rs,
+                                     reinterpret_cast<T (*)[NB + 1]>(rowbuf + kThreads * (NB + 1)),
+                                     k0, kw, sa, sb, ns, skip, cta == 0);
+            }
+            first = false;
             my_mask |= rows_below(a, Q, s, rs, rowbuf, k0, kw, sa, sb, ns, skip);
             if (my_mask) atomicOr(&cta_mask, my_mask);
             __syncthreads();
@@ -727,11 +850,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_lu_coop(CoopArgs<T> a) {
                 __syncthreads();
             }
         } else if (rest > 0) {
-            update_tiles(a, k0, kw, LUs, rowbuf);  // buffer 1 reuses the panel's buffers
-            // rows of the next block's columns above the trailing matrix are
-            // never read from P0 (positions >= nk0 only)
+            // buffer 1 reuses the panel's buffers; rows of the next block's
+            // columns above the trailing matrix are never read from P0
+            // (positions >= nk0 only)
+            update_la(a, k0, kw, kb, pass, LUs, rowbuf, s, rs,
+                      reinterpret_cast<T (*)[NB + 1]>(rowbuf + kThreads * (NB + 1)), sa, sb,
+                      &la_mask_s);
         }
-        grid_barrier(a.bar, a.flags, gen, &dead_s);
+        // FP64 form: the next pass waits for the look-ahead and strip 0 only;
+        // the pass barrier then also closes this update
+        if (kTc) grid_barrier(a.bar, a.flags, gen, &dead_s);
     }
     if (cta == 0 && tid == 0) {
         a.flags[kFlagPasses] = pass;

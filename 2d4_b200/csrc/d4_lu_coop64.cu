@@ -75,6 +75,8 @@ void factor64_async(Ctx &c, const LuBufs &L, const double *A, int grid, cudaStre
     a.flags = L.flags;
     a.bar = L.bar;
     a.perm = L.perm;
+    a.sched = L.mask + lu_pass_words((n + kLuNb - 1) / kLuNb);
+    a.dg = L.Q + (size_t)n * 64;
     void *args[] = {(void *)&a};
     D4_CUDA_OK(cudaLaunchCooperativeKernel((const void *)coop::k_lu_coop<double>, dim3(grid),
                                            dim3(coop::kThreads), args,

@@ -244,6 +244,8 @@ void factor32_async(Ctx &c, const Mix32Bufs &B, const double *A, bool copy_matri
     a.flags = B.flags;
     a.bar = B.bar;
     a.perm = B.perm;
+    a.sched = nullptr;  // the FP32 form has no look-ahead
+    a.dg = nullptr;
     void *args[] = {(void *)&a};
     const void *kern = (const void *)coop::k_lu_coop<float>;
     D4_CUDA_OK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(coop::kThreads), args,
