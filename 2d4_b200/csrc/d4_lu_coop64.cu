@@ -9,31 +9,42 @@
 // rounded separately.
 //
 // Schedule.  The matrix is processed in 32-column blocks by all CTAs of a
-// cooperative launch, separated by a grid barrier:
+// cooperative launch:
 //   pass   every CTA eliminates the block's 32 columns for its rows below the
-//          diagonal block, and all CTAs redundantly eliminate the 32x32
-//          diagonal block in shared memory, WITHOUT pivoting, starting from a
-//          saved copy P0 of the block's columns with the swaps found so far
-//          applied.  Pre-division values go to Q; a 32-bit mask records the
-//          columns where partial pivoting would have swapped (some
-//          |a_ik| > |a_kk|) or met a zero pivot.
-//   decide after the barrier every CTA reads the mask.  Empty: the pass is
-//          exact, go on.  Otherwise the first flagged column k* gets its exact
-//          pivot from Q (first max), the swap (or the singular skip) is
-//          appended to the block's list and the pass repeats.  A row swap at
-//          column k commutes with the updates of earlier columns, so applying
-//          the list to P0 up front is exact.
+//          diagonal block, WITHOUT pivoting, starting from a saved copy P0 of
+//          the block's columns with the swaps found so far applied.  The 32x32
+//          diagonal block of a block's first pass was eliminated and published
+//          by the previous update's look-ahead; for block 0 and for passes
+//          after a swap every CTA eliminates it redundantly in shared memory.
+//          Pre-division values go to Q; a 32-bit mask records the columns
+//          where partial pivoting would have swapped (some |a_ik| > |a_kk|) or
+//          met a zero pivot.  A grid barrier ends the pass.
+//   decide every CTA reads the mask.  Empty: the pass is exact, go on.
+//          Otherwise the first flagged column k* gets its exact pivot from Q
+//          (first max), the swap (or the singular skip) is appended to the
+//          block's list and the pass repeats.  A row swap at column k commutes
+//          with the updates of earlier columns, so applying the list to P0 up
+//          front is exact.
 //   finish CTAs write their rows' multipliers, apply the block's swaps to the
-//          other columns and solve U12 = L11^-1 A12 (warp per column).
-//   update trailing A22 -= L21 U12 in 64x64 tiles, the next tile's operands
-//          loaded while the current one computes; tiles that hold the next
-//          block's columns also refresh P0.  The oracle skips an update whose
-//          u_kj is exactly 0; here it is applied (x - l*0 == x for finite l, and
-//          the multipliers of an accepted pass are finite: |l| <= 1), so the
-//          factors agree bit for bit for every finite matrix.
-// A block without swaps costs one pass: three barriers per block in all.
-// Barrier waits are bounded: after kSpinLimit polls a CTA records an error
-// and stops waiting, so a launch always ends.
+//          other columns and solve U12 = L11^-1 A12 (warp per column), keeping
+//          the next diagonal block's entries (after the swaps) aside; grid
+//          barrier.
+//   update trailing A22 -= L21 U12 in 64x64 tiles on every CTA but the last,
+//          the next tile's operands loaded while the current one computes;
+//          tiles that hold the next block's columns also refresh P0 and are
+//          counted.  The last CTA forms the next diagonal block from the kept
+//          entries, L21 and U12 (the same operations in the same order as the
+//          tile that owns it), eliminates it and publishes it.  The oracle
+//          skips an update whose u_kj is exactly 0; here it is applied
+//          (x - l*0 == x for finite l, and the multipliers of an accepted pass
+//          are finite: |l| <= 1), so the factors agree bit for bit for every
+//          finite matrix.
+// The next block's first pass waits for the publication and the P0 tiles
+// only, so the update needs no grid barrier of its own and the diagonal block
+// leaves the critical path while the update runs.  A block without swaps
+// costs one pass and two grid barriers.  Every wait is bounded: after
+// kSpinLimit polls a CTA records an error and stops waiting, so a launch
+// always ends.
 #include "d4_lu_coop.cuh"
 
 namespace d4 {
