@@ -683,12 +683,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
 // no CTA waits for one that has not started.  Thread t keeps rows 2(t%64),
 // 2(t%64)+1 and columns 32(t/64).. of each tile; the next tile's slice is
 // loaded before the wait for the values it multiplies.
+//
+// Hand-off: a finished block publishes its 128 values as 64-bit words
+// (epoch << 32) | float bits, one relaxed store each, with no fence and no
+// separate flag.  A waiting warp polls the 32 words its column group needs
+// (lane l word l, 256 B per warp) until every lane sees this launch's epoch,
+// then spreads the values by shuffle: one L2 round trip per hand-off.
 struct SolveArgs {
     int n, T;
     const float *LU;
     const double *b;   // right-hand side (n)
-    float *y, *x;      // T*128 each; x is the solution
-    int *fy, *fx;      // T flags each (== epoch: block done)
+    unsigned long long *yt, *xt;  // T*128 each: tagged forward and backward values
+    float *x;          // T*128: the solution
     int *ticket;       // ticket counter (0 at the launch; the CTA taking the last ticket resets it)
     int epoch;
     int *flags;        // kFlagBarrierTimeout
@@ -696,6 +702,36 @@ struct SolveArgs {
     const unsigned long long *conv;  // refinement: max|g|, then max|r| after each sweep
     int it;            // refinement sweep of this solve
 };
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_tagged(unsigned long long *p, float v, int epoch) {
+    const unsigned long long t =
+        ((unsigned long long)(unsigned)epoch << 32) | (unsigned long long)__float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(t) : "memory");
+}
+
+// Warp-wide: lane l's value of the tagged word p[l] once all 32 words carry
+// `epoch` (bounded: after kSpin polls the wait records the timeout and the
+// values are used as they are).
+__device__ __forceinline__ float ld_tagged(const unsigned long long *p, int epoch, int *flags) {
+    const int lane = threadIdx.x & 31;
+    long long spins = 0;
+    for (;;) {
+        const unsigned long long t = ld_relaxed_u64(p + lane);
+        if (__all_sync(0xffffffffu, (unsigned)(t >> 32) == (unsigned)epoch))
+            return __uint_as_float((unsigned)t);
+        __nanosleep(32);
+        if (++spins > kSpin) {
+            if (lane == 0) gave_up(flags);
+            return __uint_as_float((unsigned)t);
+        }
+    }
+}
 
 __device__ __forceinline__ void load_slice(const SolveArgs &s, int ti, int tj, int r2, int cg,
                                            float2 (&w)[32]) {
@@ -716,8 +752,7 @@ __device__ __forceinline__ void solve_block(const SolveArgs &s, int i, float (*r
                                             float *zs) {
     const int tid = threadIdx.x, r2 = tid & 63, cg = tid >> 6;
     const int T = s.T;
-    const float *src = kFwd ? s.y : s.x;  // values of the other blocks
-    int *fl = kFwd ? s.fy : s.fx;
+    const unsigned long long *src = kFwd ? s.yt : s.xt;  // values of the other blocks
     float acc0 = 0.f, acc1 = 0.f;
     float2 w[32];
     const int k_first = kFwd ? 0 : T - 1, k_step = kFwd ? 1 : -1;
@@ -725,38 +760,30 @@ __device__ __forceinline__ void solve_block(const SolveArgs &s, int i, float (*r
     for (int q = 0; q < count; ++q) {
         const int k = k_first + q * k_step;
         load_slice(s, i, k, r2, cg, w);
-        if (tid == 0 && !wait_flag(&fl[k], s.epoch, s.flags)) gave_up(s.flags);
-        __syncthreads();
-        const float4 *yv = reinterpret_cast<const float4 *>(src + k * kB + 32 * cg);
+        // the warp's 32 values of block k (its column group), by shuffle
+        const float mine = ld_tagged(src + k * kB + 32 * cg, s.epoch, s.flags);
 #pragma unroll
-        for (int c4 = 0; c4 < 8; ++c4) {
-            const float4 yy = __ldcg(yv + c4);
-            const float ys[4] = {yy.x, yy.y, yy.z, yy.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                acc0 = fmaf(w[4 * c4 + u].x, ys[u], acc0);
-                acc1 = fmaf(w[4 * c4 + u].y, ys[u], acc1);
-            }
+        for (int cc = 0; cc < 32; ++cc) {
+            const float yy = __shfl_sync(0xffffffffu, mine, cc);
+            acc0 = fmaf(w[cc].x, yy, acc0);
+            acc1 = fmaf(w[cc].y, yy, acc1);
         }
     }
+    float base = 0.f;
     if (!kFwd) {
         load_slice(s, i, i, r2, cg, w);  // D_i, before the reduction
         // y_i comes from the forward pass of this launch
-        if (tid == 0 && !wait_flag(&s.fy[i], s.epoch, s.flags)) gave_up(s.flags);
+        if (tid < kB) base = ld_tagged(s.yt + i * kB + (tid & ~31), s.epoch, s.flags);
     }
     red[cg][2 * r2] = acc0;
     red[cg][2 * r2 + 1] = acc1;
     __syncthreads();
     if (tid < kB) {
         const int gr = i * kB + tid;
-        float base;
-        if (kFwd)
-            base = gr < s.n ? (float)s.b[s.perm ? s.perm[gr] : gr] : 0.f;
-        else
-            base = __ldcg(s.y + gr);
+        if (kFwd) base = gr < s.n ? (float)s.b[s.perm ? s.perm[gr] : gr] : 0.f;
         const float z = base - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
         if (kFwd)
-            s.y[gr] = z;
+            st_tagged(s.yt + gr, z, s.epoch);
         else
             zs[tid] = z;
     }
@@ -773,12 +800,12 @@ __device__ __forceinline__ void solve_block(const SolveArgs &s, int i, float (*r
         red[cg][2 * r2] = acc0;
         red[cg][2 * r2 + 1] = acc1;
         __syncthreads();
-        if (tid < kB)
-            s.x[i * kB + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+        if (tid < kB) {
+            const float xv = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+            s.x[i * kB + tid] = xv;
+            st_tagged(s.xt + i * kB + tid, xv, s.epoch);
+        }
     }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) st_rel(&fl[i], s.epoch);
 }
 
 // Both passes in one launch of 2T CTAs: tickets 0..T-1 are the forward pass's
@@ -859,23 +886,23 @@ void blu_alloc(BluBufs &B, int n, const int *tasks, BluState *state) {
     D4_CUDA_OK(d4::dmalloc((void **)&B.op, blu_op_bytes(n)));
     D4_CUDA_OK(d4::dmalloc((void **)&B.ticket, sizeof(int) * 4));
     D4_CUDA_OK(d4::dmalloc((void **)&B.ready, sizeof(int) * (size_t)T * T));
-    D4_CUDA_OK(d4::dmalloc((void **)&B.fy, sizeof(int) * (size_t)T));
-    D4_CUDA_OK(d4::dmalloc((void **)&B.fx, sizeof(int) * (size_t)T));
-    D4_CUDA_OK(d4::dmalloc((void **)&B.y, sizeof(float) * (size_t)T * blu::kB));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.yt, sizeof(unsigned long long) * (size_t)T * blu::kB));
+    D4_CUDA_OK(d4::dmalloc((void **)&B.xt, sizeof(unsigned long long) * (size_t)T * blu::kB));
     D4_CUDA_OK(d4::dmalloc((void **)&B.xs, sizeof(float) * (size_t)T * blu::kB));
     // ticket[0]: the factorisation's (zeroed before each launch); ticket[1]: the
     // solves' (zero here, then reset by the CTA that takes a launch's last one)
     D4_CUDA_OK(cudaMemset(B.ticket, 0, sizeof(int) * 4));
     D4_CUDA_OK(cudaMemset(B.ready, 0, sizeof(int) * (size_t)T * T));
-    D4_CUDA_OK(cudaMemset(B.fy, 0, sizeof(int) * (size_t)T));
-    D4_CUDA_OK(cudaMemset(B.fx, 0, sizeof(int) * (size_t)T));
+    // tag 0 never matches a launch's epoch (>= 1)
+    D4_CUDA_OK(cudaMemset(B.yt, 0, sizeof(unsigned long long) * (size_t)T * blu::kB));
+    D4_CUDA_OK(cudaMemset(B.xt, 0, sizeof(unsigned long long) * (size_t)T * blu::kB));
     D4_CUDA_OK(cudaMemset(B.xs, 0, sizeof(float) * (size_t)T * blu::kB));
     B.tasks = tasks;
     B.state = state;
 }
 
 void blu_free(BluBufs &B) {
-    void *p[] = {B.op, B.ticket, B.ready, B.fy, B.fx, B.y, B.xs};
+    void *p[] = {B.op, B.ticket, B.ready, B.yt, B.xt, B.xs};
     for (void *q : p)
         if (q) cudaFree(q);
     B = BluBufs();
@@ -917,10 +944,9 @@ void blu_solve_async(const BluBufs &B, int n, const float *LU, const double *b, 
     s.T = T;
     s.LU = LU;
     s.b = b;
-    s.y = B.y;
+    s.yt = B.yt;
+    s.xt = B.xt;
     s.x = B.xs;
-    s.fy = B.fy;
-    s.fx = B.fx;
     s.ticket = B.ticket + 1;
     s.epoch = ++B.state->solve_epoch;
     s.flags = flags;

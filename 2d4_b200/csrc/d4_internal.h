@@ -53,15 +53,15 @@ struct BluState {
 
 // Buffers of the mixed form's block LU and block solves (d4_blu32.cu): the
 // packed tensor-core operands of every tile (TF32 hi and lo parts), the
-// schedule, ticket counters ([0] factorisation, [1] forward, [2] backward
-// solve), the tile flags, the solves' block flags and padded vectors.
+// schedule, ticket counters ([0] factorisation, [1] the solves), the tile
+// flags, the solves' tagged block values and the solution.
 struct BluBufs {
     unsigned char *op = nullptr;
     const int *tasks = nullptr;
     int *ticket = nullptr;
     int *ready = nullptr;
-    int *fy = nullptr, *fx = nullptr;
-    float *y = nullptr, *xs = nullptr;
+    unsigned long long *yt = nullptr, *xt = nullptr;  // tagged block values of the solves
+    float *xs = nullptr;
     BluState *state = nullptr;
 };
 

@@ -123,9 +123,37 @@ __global__ void __launch_bounds__(256) k_resid_fused(int n, const double *__rest
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        double s = 0;
-        for (int c = c0; c < c1; ++c) s += __ldg(A + (size_t)i + (size_t)c * n) * sdx[c - c0];
-        part[(size_t)blockIdx.y * n + i] = s;
+        // four interleaved sums (column c into sum c % 4), combined in a fixed
+        // order: independent FMA chains, and 16 loads issued together
+        const double *Ai = A + (size_t)i + (size_t)c0 * n;
+        const int w = c1 - c0;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int c = 0;
+        for (; c + 16 <= w; c += 16) {
+            double av[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) av[u] = __ldg(Ai + (size_t)(c + u) * n);
+#pragma unroll
+            for (int u = 0; u < 16; u += 4) {
+                s0 += av[u] * sdx[c + u];
+                s1 += av[u + 1] * sdx[c + u + 1];
+                s2 += av[u + 2] * sdx[c + u + 2];
+                s3 += av[u + 3] * sdx[c + u + 3];
+            }
+        }
+        for (; c < w; ++c) {
+            const double v = __ldg(Ai + (size_t)c * n) * sdx[c];
+            const int m = c & 3;
+            if (m == 0)
+                s0 += v;
+            else if (m == 1)
+                s1 += v;
+            else if (m == 2)
+                s2 += v;
+            else
+                s3 += v;
+        }
+        part[(size_t)blockIdx.y * n + i] = (s0 + s1) + (s2 + s3);
     }
     __threadfence();
     __syncthreads();
