@@ -876,6 +876,9 @@ int d4_create(void **out, int n, const d4_params *p) {
         }
         c->use_gmres = d4::gmres_selected(*c) ? 1 : 0;
         if (c->use_gmres) d4::sparse_alloc(*c);
+        // the mixed form's dense attempts from kMixedMinN on: pair tiles
+        // without the reference's operation order (d4_fp64_fast.cu)
+        c->fast_pairs = (mixed && n >= kMixedMinN && !c->tab && !c->use_gmres) ? 1 : 0;
         if (!c->use_gmres) {
             // stage I's own stream and buffers (attempt_overlap, attempt_overlap_mixed)
             c->overlap = 1;

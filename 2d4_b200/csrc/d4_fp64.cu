@@ -113,27 +113,6 @@ inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-static PairArgs pair_args(Ctx &c, const double *x, const double *y) {
-    PairArgs a;
-    a.n = c.n;
-    a.x = x;
-    a.y = y;
-    a.F = c.F;
-    a.A = c.A;
-    a.tol = c.use_dipole ? c.tol : nullptr;
-    a.min_prec_sq = c.min_prec_sq;
-    a.h = 0;
-    a.cut_sq = c.cutoff_sq;
-    a.cutoff = c.cutoff;
-    a.range_sq = c.range_sq;
-    a.one_per_cut_sq = 1 / c.cutoff_sq;
-    a.heaviside = c.p.heaviside_cutoff;
-    a.tb.t = c.tab;
-    a.tb.T = c.tab_T;
-    a.tb.W = c.tab_T + 1 + 2 * tab::kGuard;
-    return a;
-}
-
 template <bool kJac>
 static void launch_rows(Ctx &c, const RowArgs &r, cudaStream_t st) {
     constexpr int bytes = row_smem_bytes<kJac>();
@@ -143,16 +122,14 @@ static void launch_rows(Ctx &c, const RowArgs &r, cudaStream_t st) {
     check_launch(kJac ? "k_rows64<jacobian>" : "k_rows64<speeds>");
 }
 
-static int pair_blocks(int n) {
-    const int T = (n + kTile - 1) / kTile;
-    return T * (T + 1) / 2;
-}
 
 void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
                    double ext, double *v) {
     PairArgs a = pair_args(c, x, y);
     a.F = F;
-    if (c.tab)
+    if (c.fast_pairs)
+        pairs64_fast(c, false, x, y, F, 0, st);
+    else if (c.tab)
         k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
     else
         k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
@@ -174,7 +151,9 @@ void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a
                 double *v_a, double *v_b) {
     PairArgs a = pair_args(c, x, y);
     a.h = h;
-    if (c.tab)
+    if (c.fast_pairs)
+        pairs64_fast(c, true, x, y, c.F, h, c.stream);
+    else if (c.tab)
         k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);
     else
         k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);

@@ -222,6 +222,9 @@ struct Ctx {
 
     // pair-tile autotuner (FP64 pair kernels): threads per 32x32 tile along j
     int pair_ty = 8;
+    // the mixed form's sweeps (N >= kMixedMinN, analytic field) use the pair
+    // tiles of d4_fp64_fast.cu
+    int fast_pairs = 0;
     bool pair_tuned = false;
 
     RunState rs;
@@ -299,6 +302,10 @@ void solve_update64_with(Ctx &c, const LuBufs &L, const SolveBufs &S, cudaStream
                          double hval, const double *s_end, const double *s_init,
                          const double *x_new, const double *x_old, const double *base,
                          double *out);
+// The mixed form's pair tiles (d4_fp64_fast.cu): forces into F and, for jac,
+// the raw Jacobian entries into c.A, as the plain pair tiles write them.
+void pairs64_fast(Ctx &c, bool jac, const double *x, const double *y, double *F, double h,
+                  cudaStream_t st);
 void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
                    double ext, double *v);
 // Plain solve of A dx = g (g on device, dx written to c.dx).

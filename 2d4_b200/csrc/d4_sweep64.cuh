@@ -1,7 +1,8 @@
 // d4_sweep64.cuh: the FP64 pair-sweep building blocks (pair tiles, pipelined
 // ordered row sums, row scaling), shared by the single-system engine
-// (d4_fp64.cu) and the batched ensemble (d4_ensemble.cu).  Every translation
-// unit that includes it is compiled with --fmad=false.
+// (d4_fp64.cu) and the batched ensemble (d4_ensemble.cu), which are compiled
+// with --fmad=false; d4_fp64_fast.cu builds the mixed form's pair tiles from it
+// with another field.
 //
 // Design.  The reference visits each unordered pair (i, j), i < j, once and
 // scatters its force antisymmetrically (src/simulation.cpp:292-311,444-483), so
@@ -23,6 +24,13 @@
 #include "d4_field64.cuh"
 #include "d4_internal.h"
 #include "d4_table.cuh"
+
+// The field of the pair tiles: d4::f64 (the reference's operation order) unless
+// the including file names another with the same interface (d4_fp64_fast.cu:
+// d4::f64fast for the mixed form).
+#ifndef D4_PAIR_FIELD
+#define D4_PAIR_FIELD f64
+#endif
 
 namespace d4 {
 namespace {
@@ -61,6 +69,34 @@ struct PairArgs {
     tab::Table tb;  // tabulated field (kTab kernels only)
 };
 
+// The pair sweep's arguments for a context: positions x, y, the context's
+// force matrix, Jacobian, tolerances, cutoff and table.
+inline PairArgs pair_args(const Ctx &c, const double *x, const double *y) {
+    PairArgs a;
+    a.n = c.n;
+    a.x = x;
+    a.y = y;
+    a.F = c.F;
+    a.A = c.A;
+    a.tol = c.use_dipole ? c.tol : nullptr;
+    a.min_prec_sq = c.min_prec_sq;
+    a.h = 0;
+    a.cut_sq = c.cutoff_sq;
+    a.cutoff = c.cutoff;
+    a.range_sq = c.range_sq;
+    a.one_per_cut_sq = 1 / c.cutoff_sq;
+    a.heaviside = c.p.heaviside_cutoff;
+    a.tb.t = c.tab;
+    a.tb.T = c.tab_T;
+    a.tb.W = c.tab_T + 1 + 2 * tab::kGuard;
+    return a;
+}
+
+inline int pair_blocks(int n) {
+    const int T = (n + kTile - 1) / kTile;
+    return T * (T + 1) / 2;
+}
+
 // One 32x32 tile of pairs per block; threadIdx.x = local i (coalesced column
 // stores), threadIdx.y steps local j.  kTab: the field and its x-derivative come
 // from the table (d4_table.cuh) instead of the analytic image sums.
@@ -89,8 +125,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, int tile) {
         const int j = j0 + lj;
         double f = 0, v = 0;
         if (i < a.n && j < a.n && i < j) {
-            double dx = f64::normalize(sxi[tx] - sxj[lj]);
-            double dy = f64::normalize(syi[tx] - syj[lj]);
+            double dx = D4_PAIR_FIELD::normalize(sxi[tx] - sxj[lj]);
+            double dy = D4_PAIR_FIELD::normalize(syi[tx] - syj[lj]);
             double dist_sq = dx * dx + dy * dy;
             if (a.tol && dist_sq < a.min_prec_sq) {
                 row_min = fmin(row_min, dist_sq);
@@ -103,10 +139,11 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, int tile) {
                 fxy = t.x;
                 fdx = t.y;
             } else {
-                f64::Hyp hp(f64::exp2pix(dx));
-                double c = f64::cos2piy(dy);
-                fxy = f64::xy(dx, dy, hp, c);
-                if (kJac && dist_sq < a.range_sq * a.cut_sq) fdx = f64::xy_diff_x(dx, dy, hp, c);
+                D4_PAIR_FIELD::Hyp hp(D4_PAIR_FIELD::exp2pix(dx));
+                double c = D4_PAIR_FIELD::cos2piy(dy);
+                fxy = D4_PAIR_FIELD::xy(dx, dy, hp, c);
+                if (kJac && dist_sq < a.range_sq * a.cut_sq)
+                    fdx = D4_PAIR_FIELD::xy_diff_x(dx, dy, hp, c);
             }
             f = fxy * bi * bj;
             if (kJac) {

@@ -1,10 +1,12 @@
 """GPU checks of the mixed-precision form (marked gpu).
 
-The mixed form keeps the FP64 form's sweeps, matrix, residuals, updates and
-step control, and runs the factorisations and triangular solves in FP32 (the
+The mixed form keeps FP64 sweeps, matrix, residuals, updates and step
+control, and runs the factorisations and triangular solves in FP32 (the
 block LU on the tensor cores) inside FP64 iterative refinement against the
-FP64 matrix.  Tolerances: the speeds and the matrix to 1e-12 relative of the
-oracle's (they are the FP64 form's); one attempt's positions to 1e-10; each of
+FP64 matrix.  Below N=2048 its sweeps are the FP64 form's exact-order ones;
+from N=2048 its pair tiles form each image's quotients from one reciprocal
+with product-adds contracted.  Tolerances: the speeds and the matrix to
+1e-12 relative of the oracle's; one attempt's positions to 1e-10; each of
 1000 accepted steps at N=4096, taken from the FP64 form's state, to 1e-10 of
 the FP64 form's step; 50 free-running steps to 1e-8.
 """
@@ -58,6 +60,33 @@ def test_mixed_jacobian(pkg, restated):
     vao, vbo, ao, do = restated.jacobian(x, y, 1e-4, 0.0, 0.0, cs, cut)
     assert np.abs(a - ao).max() / np.abs(ao).max() < 1e-12
     assert np.abs(d - do).max() < 1e-12
+
+
+def test_mixed_fast_sweeps(pkg, restated):
+    """From N=2048 the mixed form's pair tiles drop the reference's operation
+    order (one reciprocal per image, contracted product-adds).  Close pairs
+    give single forces of 1e5-1e6 whose row sums cancel to about 1e2, so a few
+    ulps per term show as a few 1e-12 of max|v|: speeds, the matrix and d are
+    held to 1e-10 relative of the oracle's (the exact-order sweeps of the plain
+    form meet 1e-12), and one attempt from them to 1e-10 in positions
+    (test_mixed_attempt)."""
+    n = 2048
+    x, y, _ = pkg.dconf.generate_internal(n, 1002)
+    e = engine(pkg, x, y)
+    p = restated.params()
+    mps, _, cut, cs = restated.derived(p, n)
+
+    def rel(u, w):
+        return np.abs(u - w).max() / np.abs(w).max()
+
+    v, tol = e.speeds(x, y, 0.0)
+    vo = restated.speeds(x, y, 0.0, np.full(n, mps), mps)
+    assert rel(v, vo) < 1e-10
+    va, vb, a, d, _ = e.jacobian(x, y, 1e-6, 0.0, 1e-6)
+    vao, vbo, ao, do = restated.jacobian(x, y, 1e-6, 0.0, 0.0, cs, cut)
+    assert rel(a, ao) < 1e-10
+    assert rel(d, do) < 1e-10
+    assert rel(va, vao) < 1e-10
 
 
 @pytest.mark.parametrize("n,h", [(2048, 1e-7)])
