@@ -463,6 +463,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
         const int task = *task_s;
         if (task < 0) break;
         const int i = task >> 16, j = task & 0xffff, m = min(i, j);
+        // the tile's entries of A, loaded while the accumulation runs
+        float av[64];
+        {
+            const int gr = i * kB + row;
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+                const int gc = j * kB + 64 * half + t;
+                av[t] = (gr < n && gc < n) ? a.A[(size_t)gr + (size_t)gc * n] : (gr == gc ? 1.f : 0.f);
+            }
+        }
         // ------------------------------------------------ accumulation over k < m
         if (m > 0) {
             if (warp == 0) {
@@ -514,16 +524,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_blu32(Args a) {
 #pragma unroll
             for (int t = 0; t < 64; ++t) v[t] = 0.f;
         }
-        {
-            const int gr = i * kB + row;
 #pragma unroll
-            for (int t = 0; t < 64; ++t) {
-                const int gc = j * kB + 64 * half + t;
-                const float av = (gr < n && gc < n) ? a.A[(size_t)gr + (size_t)gc * n]
-                                                    : (gr == gc ? 1.f : 0.f);
-                v[t] = av - v[t];
-            }
-        }
+        for (int t = 0; t < 64; ++t) v[t] = av[t] - v[t];
         unsigned char *slot = a.op + (size_t)(i * T + j) * kSlotBytes;
         if (i < j) {
             // U_ij = S
