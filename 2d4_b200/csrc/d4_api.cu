@@ -128,7 +128,8 @@ void free_all(Ctx *c) {
     void *ob[] = {c->lub.LU, c->lub.P0, c->lub.Q, c->lub.mask, c->lub.bar, c->lub.perm,
                   c->lub.piv, c->flags3, c->F_b, c->dvec_b, c->speed_b, c->speed2_b, c->xw1_b,
                   c->xw2_b, c->dx_b, B.A32, B.LU32, B.P0, B.Q, B.mask, B.bar, B.perm, B.piv,
-                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, B.dx2, B.cnt, B.conv, B.A64};
+                  B.g, B.r, B.dx, B.part, B.c32, B.w1, B.resid, B.dx2, B.cnt, B.conv, B.A64,
+                  c->fr_part[0], c->fr_part[1], c->fr_cnt[0], c->fr_cnt[1]};
     for (void *b : ob)
         if (b) cudaFree(b);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -879,6 +880,13 @@ int d4_create(void **out, int n, const d4_params *p) {
         // the mixed form's dense attempts from kMixedMinN on: pair tiles
         // without the reference's operation order (d4_fp64_fast.cu)
         c->fast_pairs = (mixed && n >= kMixedMinN && !c->tab && !c->use_gmres) ? 1 : 0;
+        if (c->fast_pairs)
+            for (int s = 0; s < 2; ++s) {
+                const int rb = (n + 255) / 256, nch = (n + 255) / 256;
+                dalloc(&c->fr_part[s], (size_t)2 * nch * n);
+                dalloc(&c->fr_cnt[s], (size_t)rb);
+                D4_CUDA_OK(cudaMemset(c->fr_cnt[s], 0, sizeof(unsigned) * rb));
+            }
         if (!c->use_gmres) {
             // stage I's own stream and buffers (attempt_overlap, attempt_overlap_mixed)
             c->overlap = 1;

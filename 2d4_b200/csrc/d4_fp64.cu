@@ -125,11 +125,14 @@ static void launch_rows(Ctx &c, const RowArgs &r, cudaStream_t st) {
 
 void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
                    double ext, double *v) {
+    if (c.fast_pairs) {
+        pairs64_fast(c, false, x, y, F, 0, st);
+        rows64_fast(c, false, F, ext, 0, v, nullptr, st);
+        return;
+    }
     PairArgs a = pair_args(c, x, y);
     a.F = F;
-    if (c.fast_pairs)
-        pairs64_fast(c, false, x, y, F, 0, st);
-    else if (c.tab)
+    if (c.tab)
         k_pairs64<false, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
     else
         k_pairs64<false><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, st>>>(a);
@@ -149,11 +152,17 @@ void speeds64(Ctx &c, const double *x, const double *y, double ext, double *v) {
 
 void jacobian64(Ctx &c, const double *x, const double *y, double h, double ext_a, double ext_b,
                 double *v_a, double *v_b) {
+    if (c.fast_pairs) {
+        pairs64_fast(c, true, x, y, c.F, h, c.stream);
+        rows64_fast(c, true, c.F, ext_a, ext_b, v_a, v_b, c.stream);
+        k_scale_rows64<<<blocks((long long)c.n * c.n, 256), 256, 0, c.stream>>>(c.n, c.A, c.rowsub,
+                                                                               c.rowsc);
+        check_launch("k_scale_rows64");
+        return;
+    }
     PairArgs a = pair_args(c, x, y);
     a.h = h;
-    if (c.fast_pairs)
-        pairs64_fast(c, true, x, y, c.F, h, c.stream);
-    else if (c.tab)
+    if (c.tab)
         k_pairs64<true, true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);
     else
         k_pairs64<true><<<pair_blocks(c.n), dim3(kTile, c.pair_ty), 0, c.stream>>>(a);

@@ -223,8 +223,11 @@ struct Ctx {
     // pair-tile autotuner (FP64 pair kernels): threads per 32x32 tile along j
     int pair_ty = 8;
     // the mixed form's sweeps (N >= kMixedMinN, analytic field) use the pair
-    // tiles of d4_fp64_fast.cu
+    // tiles and row sums of d4_fp64_fast.cu, with chunk partials and counters
+    // per stream ([1]: stage I's sweeps on stream_b)
     int fast_pairs = 0;
+    double *fr_part[2] = {nullptr, nullptr};
+    unsigned *fr_cnt[2] = {nullptr, nullptr};
     bool pair_tuned = false;
 
     RunState rs;
@@ -306,6 +309,9 @@ void solve_update64_with(Ctx &c, const LuBufs &L, const SolveBufs &S, cudaStream
 // the raw Jacobian entries into c.A, as the plain pair tiles write them.
 void pairs64_fast(Ctx &c, bool jac, const double *x, const double *y, double *F, double h,
                   cudaStream_t st);
+// ... and their row sums: speeds v_a (and v_b), for jac d, rowsub, rowsc.
+void rows64_fast(Ctx &c, bool jac, const double *F, double ext_a, double ext_b, double *v_a,
+                 double *v_b, cudaStream_t st);
 void speeds64_with(Ctx &c, double *F, cudaStream_t st, const double *x, const double *y,
                    double ext, double *v);
 // Plain solve of A dx = g (g on device, dx written to c.dx).
