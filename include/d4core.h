@@ -383,9 +383,10 @@ long long d4_device_allocations(void);
  * addition of this library).  For callers that cannot allocate device memory,
  * such as code running under CUDA-graph stream capture, real-time loops that
  * must not wait on an allocator, or hosts whose device memory belongs to
- * another framework's allocator.  Same result as d4_speeds of an FP64 context
- * with the analytic field (no table; the mixed form sums its pairs in another
- * order): speeds v[n] and the tolerance update of tol[n] (may be null; starts from the caller's values,
+ * another framework's allocator.  Same result as d4_speeds of a context with
+ * the analytic field (no table; every form runs the plain form's exact-order
+ * sweeps at these sizes): speeds v[n] and the tolerance update of tol[n] (may
+ * be null; starts from the caller's values,
  * clamped below min_prec_sq as PrecisionHandler::updateTolerance does) for
  * positions x[n], y[n] in internal order at external stress ext_stress.  All
  * pointers are DEVICE pointers owned by the caller; the work is queued on
